@@ -1,0 +1,323 @@
+"""Benchmark of the multi-scale DDM hot path on B200.
+
+Workload (the multi-scale FP32 configuration): 1000 frames of 1024x1024 uint8 synthetic
+Brownian-particle video (4000 Gaussian spots, sigma 2 px, amplitude 120 on background 20,
+steps N(0, 2 px^2) per axis per frame, i.e. D = 1 px^2/frame, Gaussian noise sd 4),
+scales {1024, 512, 256, 128}, 64 taus log-spaced 1..500, 30 lambdas log-spaced 2..512 px,
+tolerance 1.2, chunks of 30 frames, unbiased estimator (tau_max > chunk).
+
+One step = one chunk of 30 frames through the engine: extraction + 2-D R2C FFT of every
+tile at every scale into the device ring, then |F(t) - F(t-tau)|^2 for all 64 taus of the
+30 new frames. The ring is pre-filled with ceil(tau_max / chunk) + 1 chunks first, so every
+timed frame pairs at all 64 lags (steady state). The video is 1000 frames long and the
+steps cycle through it. The timed region ends with the azimuthal average (ISF ready).
+
+  value    frames/s with the video resident in HBM (device pointers submitted)
+  e2e      frames/s through the public API from pinned host memory: every step copies its
+           30 frames host->device and reads the updated ISF (a live result) device->host
+  roofline the lag kernel against HBM, with the algorithmic bytes per analysed frame
+           8*E*(T+1) + 16*T*E/C (one F(t) read, one F(t-tau) read per tau, Kahan
+           accumulators read+written once per chunk), E = 2,112,512 complex per frame
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "frames/s analysed (1024^2, 4 scales, 64 tau)"
+UNIT = "frames/s"
+SCALES = [1024, 512, 256, 128]
+CHUNK = 30
+N_FRAMES = 1000
+SIDE = 1024
+
+
+def workload():
+    from cuda_multiddm_b200.media import log_lambdas, log_taus
+    return log_taus(1, 500, 64), log_lambdas(2, 512, 30)
+
+
+def frames_elements() -> int:
+    return sum((SIDE // s) ** 2 * s * (s // 2 + 1) for s in SCALES)
+
+
+def lag_bytes_per_frame(T: int) -> float:
+    E = frames_elements()
+    return 8.0 * E * (T + 1) + 16.0 * T * E / CHUNK
+
+
+def make_video(seed: int, frames: int = N_FRAMES) -> np.ndarray:
+    from cuda_multiddm_b200.media import synth_video
+    return synth_video(seed, SIDE, SIDE, frames, 4000, spot_sigma=2.0, amplitude=120.0, background=20.0,
+                       step_var=2.0, noise_sd=4.0, max_value=255)
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per lag launch from the committed ncu summary (None if absent)."""
+    p = ROOT / "profiles" / "lag_kernel_c2.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi SM clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = Path("/tmp") / f"ddm_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for ln in self.path.read_text().splitlines():
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        try:
+            self.path.unlink()
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(seconds_hint: float = 20.0) -> dict:
+    """The FP64 oracle (a port of the reference's path; the reference has no CPU path)
+    timed on this host's cores, in steady state, on a bounded sample of frames."""
+    from oracle import oracle as O
+    taus, _ = workload()
+    video = make_video(1002, frames=8)
+    threads = os.cpu_count() or 1
+    # one timed frame first, then as many as fit the hint
+    t1 = O.bench_steady(video, SCALES, taus, 1, threads)
+    n = max(1, min(64, int(seconds_hint / max(t1, 1e-3))))
+    t = O.bench_steady(video, SCALES, taus, n, threads) if n > 1 else t1
+    return {"value": n / t, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} steady-state frames of the 1024^2 x 4-scale x 64-tau workload, FP64 oracle "
+                      f"(extract + R2C FFT at every scale + 64 lag pairs per frame), OpenMP {threads} threads"}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    base = cpu_baseline(seconds_hint=max(5.0, 2.0 * args.steps))
+    line = {"metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * CHUNK / base["value"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "multiscale_1024_4scales_64tau", "frames": N_FRAMES, "side": SIDE,
+                       "scales": SCALES, "taus": 64, "lambdas": 30, "chunk": CHUNK},
+            "impl": "reference", "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference has no CPU implementation of this path; its GPU build cannot run this "
+                    "configuration without reading past its accumulator allocation, so the reference arm "
+                    "is the FP64 oracle port of its algorithm on the host cores"}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    from cuda_multiddm_b200 import Engine, EngineConfig
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    taus, lambdas = workload()
+    T = len(taus)
+    video = make_video(1002 + rank)
+    dev_video = torch.from_numpy(video).cuda()
+    host_video = torch.from_numpy(video).pin_memory()
+    cfg = EngineConfig(frame_width=SIDE, frame_height=SIDE, scales=SCALES, taus=taus, lambdas=lambdas,
+                       tolerance=1.2, chunk_frames=CHUNK, estimator="unbiased", device=local)
+    eng = Engine(cfg)
+    stream = torch.cuda.ExternalStream(eng.info().stream)
+    preroll = math.ceil(max(taus) / CHUNK) + 1
+    cursor = [0]
+
+    def next_chunk():
+        i = cursor[0]
+        cursor[0] = (i + CHUNK) % (N_FRAMES - N_FRAMES % CHUNK)
+        return i
+
+    def step_device():
+        i = next_chunk()
+        eng.submit(dev_video[i:i + CHUNK])
+
+    for _ in range(preroll + args.warmup):
+        step_device()
+    eng.finalize()
+    eng.synchronize()
+
+    # ---- device-resident timed region --------------------------------------------
+    eng.set_timing(True)
+    eng.kernel_times()  # clear
+    launches0 = eng.info().kernel_launches
+    sampler = ClockSampler(local)
+    sampler.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step_device()
+    eng.finalize()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    elapsed_ms = ev0.elapsed_time(ev1)
+    ktimes = eng.kernel_times()
+    launches = eng.info().kernel_launches - launches0
+    if world > 1:
+        dist.barrier()
+
+    # ---- end to end from pinned host memory ---------------------------------------
+    eng.set_timing(False)
+    isf_host = np.zeros(eng.isf_size, np.float64)
+    from cuda_multiddm_b200._lib import check, lib
+    import ctypes as C
+
+    def step_host():
+        i = next_chunk()
+        eng.submit(host_video[i:i + CHUNK].data_ptr(), CHUNK, False)
+        check(lib().ddm_finalize(eng._h))
+        check(lib().ddm_read_isf(eng._h, isf_host.ctypes.data, isf_host.size))
+
+    for _ in range(args.warmup):
+        step_host()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step_host()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+
+    # ---- max over ranks ---------------------------------------------------------------
+    t = torch.tensor([elapsed_ms, e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    elapsed_ms, e2e_ms = float(t[0]), float(t[1])
+    frames_total = args.steps * CHUNK * world
+    value = frames_total / (elapsed_ms / 1000.0)
+    e2e_value = frames_total / (e2e_ms / 1000.0)
+
+    lag_ms, lag_n = ktimes["lag"]
+    lag_avg_s = lag_ms / 1000.0 / max(lag_n, 1)
+    bytes_per_launch = lag_bytes_per_frame(T) * CHUNK
+    hbm_peak, peak_kind = measured_peaks()
+    achieved = bytes_per_launch / lag_avg_s / 1e9
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "multiscale_1024_4scales_64tau", "frames": N_FRAMES, "side": SIDE,
+                           "scales": SCALES, "taus": T, "tau_max": max(taus), "lambdas": len(lambdas),
+                           "chunk": CHUNK, "estimator": "unbiased", "steady_state": True,
+                           "l2": "inputs larger than L2 (ring of %d frames x %.1f MB)"
+                                 % (eng.info().ring_slots, frames_elements() * 8 / 1e6),
+                           "parallelism": f"replicas x{world} (independent streams, no collective)"},
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": CHUNK * SIDE * SIDE,
+                        "d2h_bytes_per_step": isf_host.nbytes},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                             "frac": achieved / hbm_peak, "traffic": profiled_traffic(),
+                             "kernel": "lag_kernel", "peak_kind": peak_kind,
+                             "bytes_per_launch": bytes_per_launch, "avg_launch_ms": lag_avg_s * 1000.0},
+                "kernels_ms": {k: {"total_ms": v[0], "launches": v[1]} for k, v in ktimes.items()},
+                "gpu_launches": int(launches), "clocks": clocks}
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline()
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,873 @@
+// The DDM engine behind include/ddm.h: device buffers, the frame ring, scheduling of
+// the lag pairs (reference schedule or unbiased), -G snapshots and the C ABI.
+//
+// Device layout (one engine):
+//   ring   float2 [R][E]   spectra of the last R frames; frame label f lives in slot f % R.
+//                          A frame is the concatenation over scales (descending) of
+//                          [tile][ky][kx], kx in [0, s/2]; E = sum_s tiles_s * s * (s/2+1).
+//   acc    float2 [T][E]   per (tau, element): FP32 running sum of |dF|^2 and its Kahan
+//                          compensation (true value = sum - comp), unnormalised.
+//   stage  uint8  [J][M][M*bpp]   ROI of host-submitted frames (one piece at a time).
+//   tables int    [kTables][tab_stride]  lag-kernel pair tables, a ring of slots.
+//   masks  int    CSR of annulus element indices per (scale, q); counts [S][Q].
+//   isf    double [sum_s tiles_s * Q * T].
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ddm.h"
+#include "errors.hpp"
+#include "host.hpp"
+#include "kernels.cuh"
+
+namespace ddm {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+int fail(int status, const std::string &message) {
+    g_last_error = message;
+    return status;
+}
+void clear_error() { g_last_error.clear(); }
+const char *last_error() { return g_last_error.c_str(); }
+
+}  // namespace ddm
+
+using namespace ddm;
+
+namespace {
+
+constexpr int kTables = 64;  // lag tables in flight
+
+struct Launch {  // one lag-kernel launch: register frames, tau windows, position slots
+    int nreg = 0;
+    int reg[kMaxJ];
+    std::vector<int> ent_acc, ent_w, pos;
+};
+
+int log2i(long long v) {
+    int l = 0;
+    while ((1LL << l) < v) l++;
+    return l;
+}
+
+}  // namespace
+
+struct ddm_engine {
+    // configuration (sorted copies)
+    int w = 0, h = 0, bpp = 1, pixmode = 0, x_off = 0, y_off = 0;
+    std::vector<int> scales, taus;
+    std::vector<float> lambdas;
+    float tol = 1.2f;
+    int C = 30, estimator = DDM_EST_UNBIASED, multistream = 1, N = 0, G = 0, device = 0;
+    int M = 0, S = 0, T = 0, Q = 0, tau_max = 0;
+    long long E = 0;
+    std::vector<ScaleDesc> sd;
+    long long isf_size = 0;
+
+    // device state
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int R = 0, jmax = 32;
+    float2 *ring = nullptr, *acc = nullptr, *tw = nullptr;
+    uint8_t *stage = nullptr;
+    int *tables_d = nullptr, *tables_h = nullptr;
+    cudaEvent_t tab_ev[kTables] = {};
+    bool tab_used[kTables] = {};
+    int tab_stride = 0, tab_next = 0;
+    int *q_ptr_d = nullptr, *idx_d = nullptr, *counts_d = nullptr;
+    double *norm_d = nullptr, *isf_d = nullptr;
+    size_t device_bytes = 0;
+    std::vector<int> counts_h;             // [S][Q]
+    std::vector<std::vector<int>> q_ptr_s, idx_s;  // per scale CSR (host copy)
+
+    // stream state
+    long long submitted = 0;               // frame labels 0 .. submitted-1 are in (or passed) the ring
+    long long launches = 0;
+    std::vector<double> pair_count;        // unbiased: pairs per tau since the last purge
+    std::vector<CompatIteration> its;      // compat schedule
+    size_t next_it = 0;
+    int frames_read = 0;
+    bool finalized = false;
+    std::vector<std::vector<double>> dumps;
+    std::vector<double> host_norm;
+
+    // kernel timing (ddm_set_timing): event pairs and launch counts per kernel group
+    bool timing = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tev[3];
+    long tlaunch[3] = {0, 0, 0};
+};
+
+namespace {
+
+#define CUDA_TRY(expr)                                                                     \
+    do {                                                                                   \
+        cudaError_t err__ = (expr);                                                        \
+        if (err__ != cudaSuccess)                                                          \
+            return fail(err__ == cudaErrorMemoryAllocation ? DDM_ERR_OUT_OF_MEMORY : DDM_ERR_CUDA, \
+                        std::string(#expr) + ": " + cudaGetErrorString(err__));           \
+    } while (0)
+
+template <typename Tp>
+int dev_alloc(ddm_engine *e, Tp **p, size_t count) {
+    size_t bytes = sizeof(Tp) * std::max<size_t>(count, 1);
+    cudaError_t err = cudaMalloc(reinterpret_cast<void **>(p), bytes);
+    if (err != cudaSuccess)
+        return fail(DDM_ERR_OUT_OF_MEMORY, std::string("cudaMalloc of ") + std::to_string(bytes) +
+                                               " bytes failed: " + cudaGetErrorString(err));
+    e->device_bytes += bytes;
+    return DDM_OK;
+}
+
+void free_all(ddm_engine *e) {
+    cudaFree(e->ring);
+    cudaFree(e->acc);
+    cudaFree(e->tw);
+    cudaFree(e->stage);
+    cudaFree(e->tables_d);
+    cudaFree(e->q_ptr_d);
+    cudaFree(e->idx_d);
+    cudaFree(e->counts_d);
+    cudaFree(e->norm_d);
+    cudaFree(e->isf_d);
+    if (e->tables_h) cudaFreeHost(e->tables_h);
+    for (int i = 0; i < kTables; i++)
+        if (e->tab_ev[i]) cudaEventDestroy(e->tab_ev[i]);
+    for (int g = 0; g < 3; g++)
+        for (auto &pr : e->tev[g]) {
+            cudaEventDestroy(pr.first);
+            cudaEventDestroy(pr.second);
+        }
+    if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
+}
+
+// Brackets a group of launches with events when timing is on (group 0 FFT, 1 lag, 2 azimuth).
+struct TimedRange {
+    ddm_engine *e;
+    int group;
+    cudaEvent_t start = nullptr;
+    TimedRange(ddm_engine *e_, int g) : e(e_), group(g) {
+        if (e->timing && cudaEventCreate(&start) == cudaSuccess) cudaEventRecord(start, e->stream);
+    }
+    void end(long launches) {
+        e->tlaunch[group] += launches;
+        if (!start) return;
+        cudaEvent_t stop;
+        if (cudaEventCreate(&stop) == cudaSuccess) {
+            cudaEventRecord(stop, e->stream);
+            e->tev[group].push_back({start, stop});
+        } else {
+            cudaEventDestroy(start);
+        }
+        start = nullptr;
+    }
+};
+
+// ---------------------------------------------------------------------------------
+// FFT of a piece of frames into ring slots (first_label + f) % R
+// ---------------------------------------------------------------------------------
+
+int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long long row_pitch,
+               int x_off, int y_off, int nframes, long long first_label) {
+    const int log2tw = log2i(e->scales[0]);
+    TimedRange tr(e, 0);
+    for (const ScaleDesc &d : e->sd) {
+        const int s = d.s, log2s = log2i(s);
+        RowArgs ra;
+        ra.src = src;
+        ra.frame_stride = frame_stride;
+        ra.row_pitch = row_pitch;
+        ra.bpp = e->bpp;
+        ra.pixmode = e->pixmode;
+        ra.x_off = x_off;
+        ra.y_off = y_off;
+        ra.s = s;
+        ra.log2s = log2s;
+        ra.tiles_side = e->M / s;
+        ra.pairs_per_cta = std::max(1, std::min(s / 2, 2048 / s));
+        ra.ctas_per_tile = (s / 2) / ra.pairs_per_cta;
+        ra.n = d.n;
+        ra.off = d.off;
+        ra.E = e->E;
+        ra.first_label = first_label;
+        ra.R = e->R;
+        ra.ring = e->ring;
+        ra.tw = e->tw;
+        ra.log2tw = log2tw;
+        dim3 grid(d.tiles * ra.ctas_per_tile, nframes);
+        size_t smem = sizeof(float2) * ra.pairs_per_cta * s;
+        fft_rows_kernel<<<grid, kFftThreads, smem, e->stream>>>(ra);
+        CUDA_TRY(cudaGetLastError());
+        e->launches++;
+
+        ColArgs ca;
+        ca.s = s;
+        ca.log2s = log2s;
+        ca.P = std::min(16, std::max(1, 16384 / s));
+        ca.groups_per_tile = (s / 2 + 1 + ca.P - 1) / ca.P;
+        ca.n = d.n;
+        ca.off = d.off;
+        ca.E = e->E;
+        ca.first_label = first_label;
+        ca.R = e->R;
+        ca.ring = e->ring;
+        ca.tw = e->tw;
+        ca.log2tw = log2tw;
+        dim3 cgrid(d.tiles * ca.groups_per_tile, nframes);
+        size_t csmem = sizeof(float2) * ca.P * s;
+        fft_cols_kernel<<<cgrid, kFftThreads, csmem, e->stream>>>(ca);
+        CUDA_TRY(cudaGetLastError());
+        e->launches++;
+    }
+    tr.end(2L * e->S);
+    return DDM_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// Lag launches
+// ---------------------------------------------------------------------------------
+
+int launch_lag(ddm_engine *e, const Launch &L) {
+    if (L.nreg <= 0 || L.ent_acc.empty()) return DDM_OK;
+    const int ntau = static_cast<int>(L.ent_acc.size());
+    const int npos = static_cast<int>(L.pos.size());
+    const int ntab = kTabEntries + 2 * ntau + npos;
+    if (ntab > e->tab_stride) return fail(DDM_ERR_STATE, "internal: lag table overflow");
+    const int ts = e->tab_next;
+    e->tab_next = (e->tab_next + 1) % kTables;
+    if (e->tab_used[ts]) CUDA_TRY(cudaEventSynchronize(e->tab_ev[ts]));
+    int *th = e->tables_h + static_cast<size_t>(ts) * e->tab_stride;
+    th[kTabNreg] = L.nreg;
+    th[kTabNtau] = ntau;
+    th[kTabNpos] = npos;
+    for (int j = 0; j < kMaxJ; j++) th[kTabReg + j] = j < L.nreg ? L.reg[j] : -1;
+    std::copy(L.ent_acc.begin(), L.ent_acc.end(), th + kTabEntries);
+    std::copy(L.ent_w.begin(), L.ent_w.end(), th + kTabEntries + ntau);
+    std::copy(L.pos.begin(), L.pos.end(), th + kTabEntries + 2 * ntau);
+    int *td = e->tables_d + static_cast<size_t>(ts) * e->tab_stride;
+    CUDA_TRY(cudaMemcpyAsync(td, th, sizeof(int) * ntab, cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(cudaEventRecord(e->tab_ev[ts], e->stream));
+    e->tab_used[ts] = true;
+
+    const unsigned blocks = static_cast<unsigned>((e->E + kLagThreads - 1) / kLagThreads);
+    const size_t smem = sizeof(int) * ntab;
+    TimedRange tr(e, 1);
+    if (L.nreg <= 8)
+        lag_kernel<8><<<blocks, kLagThreads, smem, e->stream>>>(e->ring, e->acc, e->E, td);
+    else if (L.nreg <= 16)
+        lag_kernel<16><<<blocks, kLagThreads, smem, e->stream>>>(e->ring, e->acc, e->E, td);
+    else
+        lag_kernel<32><<<blocks, kLagThreads, smem, e->stream>>>(e->ring, e->acc, e->E, td);
+    CUDA_TRY(cudaGetLastError());
+    tr.end(1);
+    e->launches++;
+    return DDM_OK;
+}
+
+inline int slot_of(const ddm_engine *e, long long label) {
+    return label < 0 ? -1 : static_cast<int>(label % e->R);
+}
+
+// Unbiased: the new frames n0 .. n0+c-1 pair with the frames tau before each.
+int lag_causal(ddm_engine *e, long long n0, int c) {
+    Launch L;
+    L.nreg = c;
+    for (int j = 0; j < c; j++) L.reg[j] = slot_of(e, n0 + j);
+    for (int i = e->T - 1; i >= 0; i--) {  // descending tau = ascending window start
+        L.ent_acc.push_back(i);
+        L.ent_w.push_back(e->tau_max - e->taus[i]);
+        long long first = n0 - e->taus[i];  // partner of j = 0
+        long long valid = std::max<long long>(0, std::min<long long>(c, first + c));
+        e->pair_count[i] += static_cast<double>(valid);
+    }
+    L.pos.resize(c + e->tau_max);
+    for (int p = 0; p < c + e->tau_max; p++) {
+        long long f = n0 - e->tau_max + p;
+        L.pos[p] = f >= 0 ? slot_of(e, f) : -1;
+    }
+    return launch_lag(e, L);
+}
+
+// Reference schedule: iteration `it` pairs A = start[fo] with position fo + tau of
+// start|end (src/DDM.cu:250-255).
+int lag_iteration(ddm_engine *e, const CompatIteration &it) {
+    for (int f0 = 0; f0 < it.count; f0 += kMaxJ) {
+        Launch L;
+        L.nreg = std::min(kMaxJ, it.count - f0);
+        for (int j = 0; j < L.nreg; j++) L.reg[j] = slot_of(e, it.start[f0 + j]);
+        for (int i = 0; i < e->T; i++) {
+            L.ent_acc.push_back(i);
+            L.ent_w.push_back(e->taus[i]);
+        }
+        L.pos.resize(L.nreg + e->tau_max);
+        for (int p = 0; p < L.nreg + e->tau_max; p++) {
+            const int q = f0 + p;
+            int lab = q < e->C ? it.start[q] : (q - e->C < e->C ? it.end[q - e->C] : kLabelUninit);
+            L.pos[p] = slot_of(e, lab);
+        }
+        int st = launch_lag(e, L);
+        if (st) return st;
+    }
+    return DDM_OK;
+}
+
+int run_azimuth(ddm_engine *e, const std::vector<double> &norm) {
+    CUDA_TRY(cudaMemcpyAsync(e->norm_d, norm.data(), sizeof(double) * e->T, cudaMemcpyHostToDevice,
+                             e->stream));
+    // the copy reads host memory asynchronously: keep the source alive until it ran
+    e->host_norm = norm;
+    AzArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.S = e->S;
+    a.T = e->T;
+    a.Q = e->Q;
+    int blocks = 0;
+    for (int s = 0; s < e->S; s++) {
+        a.sc[s] = e->sd[s];
+        a.block_prefix[s] = blocks;
+        blocks += e->sd[s].tiles * e->T;
+    }
+    a.block_prefix[e->S] = blocks;
+    a.acc = e->acc;
+    a.E = e->E;
+    a.q_ptr = e->q_ptr_d;
+    a.idx = e->idx_d;
+    a.counts = e->counts_d;
+    a.norm = e->norm_d;
+    a.isf = e->isf_d;
+    TimedRange tr(e, 2);
+    azimuth_kernel<<<blocks, kAzThreads, 0, e->stream>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    tr.end(1);
+    e->launches++;
+    // pageable source: make sure the copy has consumed host_norm before it can change
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return DDM_OK;
+}
+
+int purge(ddm_engine *e) {
+    CUDA_TRY(cudaMemsetAsync(e->acc, 0, sizeof(float2) * e->T * e->E, e->stream));
+    std::fill(e->pair_count.begin(), e->pair_count.end(), 0.0);
+    return DDM_OK;
+}
+
+int snapshot(ddm_engine *e, const std::vector<double> &norm) {
+    int st = run_azimuth(e, norm);
+    if (st) return st;
+    std::vector<double> out(e->isf_size);
+    CUDA_TRY(cudaMemcpy(out.data(), e->isf_d, sizeof(double) * e->isf_size, cudaMemcpyDeviceToHost));
+    e->dumps.push_back(std::move(out));
+    return purge(e);
+}
+
+// Compat: run every pending iteration whose frames have all been submitted.
+int run_ready_iterations(ddm_engine *e, bool final_pass) {
+    while (e->next_it < e->its.size()) {
+        const CompatIteration &it = e->its[e->next_it];
+        if (it.max_label >= e->submitted) {
+            if (!final_pass) break;
+            return fail(DDM_ERR_NEED_FRAMES, "the reference schedule reads frame " +
+                                                 std::to_string(it.max_label) + " but only " +
+                                                 std::to_string(e->submitted) + " were submitted");
+        }
+        if (it.min_label < e->submitted - e->R)
+            return fail(DDM_ERR_STATE, "internal: ring too small for the reference schedule");
+        int st = lag_iteration(e, it);
+        if (st) return st;
+        e->next_it++;
+        if (it.dump_after) {
+            std::vector<double> norm(e->T, static_cast<double>(e->C) * e->G);  // src/DDM.cu:808
+            st = snapshot(e, norm);
+            if (st) return st;
+        }
+    }
+    return DDM_OK;
+}
+
+}  // namespace
+
+// =================================================================================
+// C ABI
+// =================================================================================
+
+extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
+    clear_error();
+    if (!cfg || !out) return fail(DDM_ERR_INVALID_ARG, "ddm_open: null argument");
+    *out = nullptr;
+    if (!cfg->scales || !cfg->taus || !cfg->lambdas || cfg->scale_count <= 0 || cfg->tau_count <= 0 ||
+        cfg->lambda_count <= 0)
+        return fail(DDM_ERR_INVALID_ARG, "scale, tau and lambda lists must each hold at least one value");
+    if (cfg->scale_count > kMaxScales)
+        return fail(DDM_ERR_INVALID_ARG, "at most " + std::to_string(kMaxScales) + " scales");
+    if (cfg->bytes_per_pixel != 1 && cfg->bytes_per_pixel != 2)
+        return fail(DDM_ERR_INVALID_ARG, "bytes_per_pixel must be 1 or 2");
+    if (cfg->pixel_mode == DDM_PIX_U16LE && cfg->bytes_per_pixel != 2)
+        return fail(DDM_ERR_INVALID_ARG, "DDM_PIX_U16LE needs bytes_per_pixel = 2");
+    if (cfg->pixel_mode != DDM_PIX_BYTE0 && cfg->pixel_mode != DDM_PIX_U16LE)
+        return fail(DDM_ERR_INVALID_ARG, "unknown pixel_mode");
+    if (cfg->estimator != DDM_EST_COMPAT && cfg->estimator != DDM_EST_UNBIASED)
+        return fail(DDM_ERR_INVALID_ARG, "unknown estimator");
+
+    ddm_engine *e = new ddm_engine;
+    e->w = cfg->frame_width;
+    e->h = cfg->frame_height;
+    e->bpp = cfg->bytes_per_pixel;
+    e->pixmode = cfg->pixel_mode;
+    e->x_off = cfg->x_offset;
+    e->y_off = cfg->y_offset;
+    e->scales.assign(cfg->scales, cfg->scales + cfg->scale_count);
+    e->taus.assign(cfg->taus, cfg->taus + cfg->tau_count);
+    e->lambdas.assign(cfg->lambdas, cfg->lambdas + cfg->lambda_count);
+    std::sort(e->taus.begin(), e->taus.end());  // src/DDM.cu:319-321
+    std::sort(e->lambdas.begin(), e->lambdas.end());
+    std::sort(e->scales.begin(), e->scales.end(), std::greater<int>());
+    e->tol = cfg->tolerance;
+    e->C = cfg->chunk_frames;
+    e->estimator = cfg->estimator;
+    e->multistream = cfg->multistream ? 1 : 0;
+    e->N = cfg->total_frames;
+    e->G = cfg->dump_every;
+    e->device = cfg->device;
+    const bool compat = e->estimator == DDM_EST_COMPAT;
+
+    auto bail = [&](int st) {
+        free_all(e);
+        delete e;
+        return st;
+    };
+    std::string msg = validate_reference_params(e->scales, e->taus, e->lambdas, e->tol, e->C,
+                                                /*enforce_tau_chunk=*/compat,
+                                                /*enforce_lambda_scale=*/compat, nullptr);
+    if (!msg.empty()) return bail(fail(DDM_ERR_INVALID_ARG, msg));
+    e->M = e->scales[0];
+    if (e->M > 16384) return bail(fail(DDM_ERR_INVALID_ARG, "the largest scale must be <= 16384"));
+    if (e->M + e->x_off > e->w || e->M + e->y_off > e->h || e->x_off < 0 || e->y_off < 0)
+        return bail(fail(DDM_ERR_INVALID_ARG, "the specified out dimensions must be smaller than actual image size"));
+    if (e->scales.back() < 2) return bail(fail(DDM_ERR_INVALID_ARG, "scales must be at least 2"));
+    if (e->G < 0) return bail(fail(DDM_ERR_INVALID_ARG, "dump_every must be >= 0"));
+    if (compat && e->N <= 0) return bail(fail(DDM_ERR_INVALID_ARG, "the reference schedule needs total_frames > 0"));
+    e->S = static_cast<int>(e->scales.size());
+    e->T = static_cast<int>(e->taus.size());
+    e->Q = static_cast<int>(e->lambdas.size());
+    e->tau_max = e->taus.back();
+    if (e->tau_max > 40000 || e->T > 8192)
+        return bail(fail(DDM_ERR_INVALID_ARG, "tau_max must be <= 40000 and at most 8192 taus"));
+
+    // Geometry
+    long long off = 0, isf_off = 0;
+    int q_base = 0;
+    for (int s : e->scales) {
+        ScaleDesc d;
+        d.s = s;
+        d.tiles = (e->M / s) * (e->M / s);
+        d.n = static_cast<long long>(s) * (s / 2 + 1);
+        d.off = off;
+        d.isf_off = isf_off;
+        d.q_base = q_base;
+        d.inv_s4 = 1.0 / (static_cast<double>(s) * s * static_cast<double>(s) * s);
+        off += d.tiles * d.n;
+        isf_off += static_cast<long long>(d.tiles) * e->Q * e->T;
+        q_base += e->Q;
+        e->sd.push_back(d);
+    }
+    e->E = off;
+    e->isf_size = isf_off;
+
+    // Schedule and ring size
+    e->jmax = std::min(kMaxJ, e->C);
+    if (compat) {
+        e->its = compat_schedule(e->N, e->C, e->multistream, e->G, e->taus, &e->frames_read);
+        // Frames arrive in pieces of jmax and iterations run in order, each once every
+        // frame it reads is in: iteration j runs when at most run_j + jmax frames have
+        // been submitted (run_j = the largest label read by iterations 0..j), so the ring
+        // must still hold its oldest label then.
+        int span = 1, run = -1;
+        for (const CompatIteration &it : e->its) {
+            run = std::max(run, it.max_label);
+            if (it.max_label >= 0) span = std::max(span, run + e->jmax - it.min_label + 1);
+        }
+        e->R = span;
+    } else {
+        e->R = e->tau_max + e->jmax;
+        e->pair_count.assign(e->T, 0.0);
+    }
+
+    // Budget check before any allocation
+    const size_t ring_bytes = sizeof(float2) * static_cast<size_t>(e->R) * e->E;
+    const size_t acc_bytes = sizeof(float2) * static_cast<size_t>(e->T) * e->E;
+    const size_t stage_bytes = static_cast<size_t>(e->jmax) * e->M * e->M * e->bpp;
+    e->tab_stride = kTabEntries + 2 * e->T + kMaxJ + e->tau_max + 4;
+    size_t need = ring_bytes + acc_bytes + stage_bytes + sizeof(double) * e->isf_size +
+                  sizeof(int) * static_cast<size_t>(kTables) * e->tab_stride;
+    if (cfg->hbm_budget_bytes && need > cfg->hbm_budget_bytes)
+        return bail(fail(DDM_ERR_OUT_OF_MEMORY, "engine needs " + std::to_string(need) +
+                                                    " device bytes, over the budget of " +
+                                                    std::to_string(cfg->hbm_budget_bytes)));
+
+    // Device
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= e->device || e->device < 0)
+        return bail(fail(DDM_ERR_NO_DEVICE, "no CUDA device " + std::to_string(e->device)));
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, e->device) != cudaSuccess || prop.major != 10)
+        return bail(fail(DDM_ERR_NO_DEVICE, "device " + std::to_string(e->device) + " is not an sm_100 GPU"));
+    if (cudaSetDevice(e->device) != cudaSuccess) return bail(fail(DDM_ERR_CUDA, "cudaSetDevice failed"));
+    if (cfg->stream) {
+        e->stream = static_cast<cudaStream_t>(cfg->stream);
+    } else {
+        if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess)
+            return bail(fail(DDM_ERR_CUDA, "cudaStreamCreate failed"));
+        e->own_stream = true;
+    }
+    int st;
+    if ((st = dev_alloc(e, &e->ring, static_cast<size_t>(e->R) * e->E))) return bail(st);
+    if ((st = dev_alloc(e, &e->acc, static_cast<size_t>(e->T) * e->E))) return bail(st);
+    if ((st = dev_alloc(e, &e->stage, stage_bytes))) return bail(st);
+    if ((st = dev_alloc(e, &e->tables_d, static_cast<size_t>(kTables) * e->tab_stride))) return bail(st);
+    if ((st = dev_alloc(e, &e->norm_d, e->T))) return bail(st);
+    if ((st = dev_alloc(e, &e->isf_d, e->isf_size))) return bail(st);
+    if (cudaMallocHost(reinterpret_cast<void **>(&e->tables_h),
+                       sizeof(int) * static_cast<size_t>(kTables) * e->tab_stride) != cudaSuccess)
+        return bail(fail(DDM_ERR_OUT_OF_MEMORY, "pinned table buffer"));
+    for (int i = 0; i < kTables; i++)
+        if (cudaEventCreateWithFlags(&e->tab_ev[i], cudaEventDisableTiming) != cudaSuccess)
+            return bail(fail(DDM_ERR_CUDA, "cudaEventCreate failed"));
+
+    // Twiddles e^{-2 pi i m / M}, m < M/2, from FP64 math rounded to FP32
+    {
+        std::vector<float2> tw(std::max(1, e->M / 2));
+        const double two_pi = 6.283185307179586476925286766559;
+        for (int m = 0; m < e->M / 2; m++) {
+            double a = two_pi * m / e->M;
+            tw[m] = make_float2(static_cast<float>(std::cos(a)), static_cast<float>(-std::sin(a)));
+        }
+        if ((st = dev_alloc(e, &e->tw, tw.size()))) return bail(st);
+        if (cudaMemcpy(e->tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+            return bail(fail(DDM_ERR_CUDA, "twiddle upload failed"));
+    }
+
+    // Masks (bit-exact host construction) as CSR per (scale, q)
+    {
+        std::vector<int> q_ptr_all, idx_all;
+        for (int s = 0; s < e->S; s++) {
+            std::vector<int> qp, idx, counts;
+            build_masks(e->scales[s], e->lambdas, e->tol, &qp, &idx, &counts);
+            const int base = static_cast<int>(idx_all.size());
+            for (int q = 0; q <= e->Q; q++) q_ptr_all.push_back(base + qp[q]);
+            idx_all.insert(idx_all.end(), idx.begin(), idx.end());
+            e->counts_h.insert(e->counts_h.end(), counts.begin(), counts.end());
+            e->q_ptr_s.push_back(qp);
+            e->idx_s.push_back(std::move(idx));
+        }
+        if ((st = dev_alloc(e, &e->q_ptr_d, q_ptr_all.size()))) return bail(st);
+        if ((st = dev_alloc(e, &e->idx_d, idx_all.size()))) return bail(st);
+        if ((st = dev_alloc(e, &e->counts_d, e->counts_h.size()))) return bail(st);
+        if (cudaMemcpy(e->q_ptr_d, q_ptr_all.data(), sizeof(int) * q_ptr_all.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+            (!idx_all.empty() && cudaMemcpy(e->idx_d, idx_all.data(), sizeof(int) * idx_all.size(), cudaMemcpyHostToDevice) != cudaSuccess) ||
+            cudaMemcpy(e->counts_d, e->counts_h.data(), sizeof(int) * e->counts_h.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+            return bail(fail(DDM_ERR_CUDA, "mask upload failed"));
+    }
+
+    // Kernel shared-memory limits (the FFT passes use up to 128 KB)
+    if (cudaFuncSetAttribute(fft_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024) != cudaSuccess ||
+        cudaFuncSetAttribute(fft_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024) != cudaSuccess ||
+        cudaFuncSetAttribute(lag_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess ||
+        cudaFuncSetAttribute(lag_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess ||
+        cudaFuncSetAttribute(lag_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
+        return bail(fail(DDM_ERR_CUDA, "cudaFuncSetAttribute failed"));
+    if (sizeof(int) * e->tab_stride > 200 * 1024)
+        return bail(fail(DDM_ERR_INVALID_ARG, "tau list too long for the lag table"));
+
+    if (cudaMemsetAsync(e->acc, 0, acc_bytes, e->stream) != cudaSuccess ||
+        cudaMemsetAsync(e->ring, 0, ring_bytes, e->stream) != cudaSuccess ||
+        cudaStreamSynchronize(e->stream) != cudaSuccess)
+        return bail(fail(DDM_ERR_CUDA, "initial memset failed"));
+    *out = e;
+    return DDM_OK;
+}
+
+extern "C" int ddm_close(ddm_engine *e) {
+    if (!e) return DDM_OK;
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    free_all(e);
+    delete e;
+    return DDM_OK;
+}
+
+extern "C" int ddm_submit_frames(ddm_engine *e, const void *frames, int count, int on_device) {
+    clear_error();
+    if (!e || (!frames && count > 0) || count < 0) return fail(DDM_ERR_INVALID_ARG, "ddm_submit_frames: bad argument");
+    const bool compat = e->estimator == DDM_EST_COMPAT;
+    if (compat && e->finalized) return fail(DDM_ERR_STATE, "engine already finalized");
+    if (compat && e->submitted + count > e->frames_read)
+        return fail(DDM_ERR_STATE, "the reference schedule reads only " + std::to_string(e->frames_read) + " frames");
+    const size_t frame_bytes = static_cast<size_t>(e->w) * e->h * e->bpp;
+    const uint8_t *src = static_cast<const uint8_t *>(frames);
+    int done = 0;
+    while (done < count) {
+        int piece = std::min(count - done, e->jmax);
+        if (!compat && e->G > 0) {  // unbiased -G: cut pieces at snapshot boundaries
+            const long long period = static_cast<long long>(e->G) * e->C;
+            const long long to_edge = period - e->submitted % period;
+            piece = static_cast<int>(std::min<long long>(piece, to_edge));
+        }
+        const uint8_t *p = src + frame_bytes * done;
+        int st;
+        if (on_device) {
+            st = launch_fft(e, p, static_cast<long long>(frame_bytes), static_cast<long long>(e->w) * e->bpp,
+                            e->x_off, e->y_off, piece, e->submitted);
+        } else {
+            const size_t roi_row = static_cast<size_t>(e->M) * e->bpp;
+            for (int f = 0; f < piece; f++) {
+                const uint8_t *fp = p + frame_bytes * f +
+                                    (static_cast<size_t>(e->y_off) * e->w + e->x_off) * e->bpp;
+                CUDA_TRY(cudaMemcpy2DAsync(e->stage + static_cast<size_t>(f) * e->M * roi_row, roi_row, fp,
+                                           static_cast<size_t>(e->w) * e->bpp, roi_row, e->M,
+                                           cudaMemcpyHostToDevice, e->stream));
+            }
+            st = launch_fft(e, e->stage, static_cast<long long>(e->M) * roi_row, static_cast<long long>(roi_row),
+                            0, 0, piece, e->submitted);
+        }
+        if (st) return st;
+        const long long n0 = e->submitted;
+        e->submitted += piece;
+        if (compat) {
+            if ((st = run_ready_iterations(e, false))) return st;
+        } else {
+            if ((st = lag_causal(e, n0, piece))) return st;
+            if (e->G > 0 && e->submitted % (static_cast<long long>(e->G) * e->C) == 0) {
+                if ((st = snapshot(e, e->pair_count))) return st;
+            }
+        }
+        done += piece;
+    }
+    return DDM_OK;
+}
+
+extern "C" int ddm_finalize(ddm_engine *e) {
+    clear_error();
+    if (!e) return fail(DDM_ERR_INVALID_ARG, "ddm_finalize: null engine");
+    int st;
+    std::vector<double> norm(e->T);
+    if (e->estimator == DDM_EST_COMPAT) {
+        if (e->finalized) return fail(DDM_ERR_STATE, "engine already finalized");
+        if ((st = run_ready_iterations(e, true))) return st;
+        std::fill(norm.begin(), norm.end(), static_cast<double>(e->N));  // src/DDM.cu:875
+    } else {
+        norm = e->pair_count;
+    }
+    if ((st = run_azimuth(e, norm))) return st;
+    e->finalized = true;
+    return DDM_OK;
+}
+
+extern "C" long ddm_isf_size(const ddm_engine *e) { return e ? static_cast<long>(e->isf_size) : 0; }
+
+extern "C" int ddm_read_isf(ddm_engine *e, double *out, long capacity) {
+    clear_error();
+    if (!e || !out || capacity < e->isf_size) return fail(DDM_ERR_INVALID_ARG, "ddm_read_isf: bad argument");
+    if (!e->finalized) return fail(DDM_ERR_STATE, "ddm_finalize has not run");
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    CUDA_TRY(cudaMemcpy(out, e->isf_d, sizeof(double) * e->isf_size, cudaMemcpyDeviceToHost));
+    return DDM_OK;
+}
+
+extern "C" int ddm_dump_count(const ddm_engine *e) { return e ? static_cast<int>(e->dumps.size()) : 0; }
+
+extern "C" int ddm_read_dump(ddm_engine *e, int index, double *out, long capacity) {
+    clear_error();
+    if (!e || !out || index < 0 || index >= static_cast<int>(e->dumps.size()) || capacity < e->isf_size)
+        return fail(DDM_ERR_INVALID_ARG, "ddm_read_dump: bad argument");
+    std::copy(e->dumps[index].begin(), e->dumps[index].end(), out);
+    return DDM_OK;
+}
+
+extern "C" int ddm_reset_accumulators(ddm_engine *e) {
+    clear_error();
+    if (!e) return fail(DDM_ERR_INVALID_ARG, "null engine");
+    return purge(e);
+}
+
+extern "C" int ddm_synchronize(ddm_engine *e) {
+    clear_error();
+    if (!e) return fail(DDM_ERR_INVALID_ARG, "null engine");
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    CUDA_TRY(cudaGetLastError());
+    return DDM_OK;
+}
+
+extern "C" int ddm_get_params(const ddm_engine *e, int *scales, int *taus, float *lambdas) {
+    if (!e) return fail(DDM_ERR_INVALID_ARG, "null engine");
+    if (scales) std::copy(e->scales.begin(), e->scales.end(), scales);
+    if (taus) std::copy(e->taus.begin(), e->taus.end(), taus);
+    if (lambdas) std::copy(e->lambdas.begin(), e->lambdas.end(), lambdas);
+    return DDM_OK;
+}
+
+extern "C" int ddm_get_pixel_counts(const ddm_engine *e, int *counts) {
+    if (!e || !counts) return fail(DDM_ERR_INVALID_ARG, "bad argument");
+    std::copy(e->counts_h.begin(), e->counts_h.end(), counts);
+    return DDM_OK;
+}
+
+extern "C" int ddm_get_mask(const ddm_engine *e, int si, unsigned char *mask, long capacity) {
+    if (!e || !mask || si < 0 || si >= e->S) return fail(DDM_ERR_INVALID_ARG, "bad argument");
+    const long long n = e->sd[si].n;
+    if (capacity < n * e->Q) return fail(DDM_ERR_INVALID_ARG, "mask buffer too small");
+    std::memset(mask, 0, static_cast<size_t>(n * e->Q));
+    for (int q = 0; q < e->Q; q++)
+        for (int i = e->q_ptr_s[si][q]; i < e->q_ptr_s[si][q + 1]; i++) mask[q * n + e->idx_s[si][i]] = 1;
+    return DDM_OK;
+}
+
+extern "C" long ddm_frame_elements(const ddm_engine *e) { return e ? static_cast<long>(e->E) : 0; }
+
+extern "C" int ddm_read_spectrum(ddm_engine *e, int frame, float *out, long capacity) {
+    clear_error();
+    if (!e || !out || capacity < 2 * e->E) return fail(DDM_ERR_INVALID_ARG, "bad argument");
+    if (frame < 0 || frame >= e->submitted || frame < e->submitted - e->R)
+        return fail(DDM_ERR_INVALID_ARG, "frame is not in the ring");
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    CUDA_TRY(cudaMemcpy(out, e->ring + static_cast<size_t>(frame % e->R) * e->E, sizeof(float2) * e->E,
+                        cudaMemcpyDeviceToHost));
+    return DDM_OK;
+}
+
+extern "C" int ddm_read_accumulators(ddm_engine *e, double *out, long capacity) {
+    clear_error();
+    if (!e || !out || capacity < static_cast<long>(e->T * e->E)) return fail(DDM_ERR_INVALID_ARG, "bad argument");
+    std::vector<float2> tmp(static_cast<size_t>(e->T) * e->E);
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    CUDA_TRY(cudaMemcpy(tmp.data(), e->acc, sizeof(float2) * tmp.size(), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < tmp.size(); i++) out[i] = static_cast<double>(tmp[i].x) - static_cast<double>(tmp[i].y);
+    return DDM_OK;
+}
+
+extern "C" int ddm_get_info(const ddm_engine *e, ddm_info *info) {
+    if (!e || !info) return fail(DDM_ERR_INVALID_ARG, "bad argument");
+    info->frames_submitted = static_cast<long>(e->submitted);
+    info->ring_slots = e->R;
+    info->device_bytes = e->device_bytes;
+    info->kernel_launches = static_cast<long>(e->launches);
+    info->stream = e->stream;
+    info->frames_needed = e->estimator == DDM_EST_COMPAT ? e->frames_read : 0;
+    return DDM_OK;
+}
+
+extern "C" const char *ddm_last_error(void) { return last_error(); }
+
+extern "C" int ddm_set_timing(ddm_engine *e, int enabled) {
+    if (!e) return fail(DDM_ERR_INVALID_ARG, "null engine");
+    e->timing = enabled != 0;
+    return DDM_OK;
+}
+
+extern "C" int ddm_kernel_times(ddm_engine *e, double *ms, long *launches) {
+    clear_error();
+    if (!e || !ms || !launches) return fail(DDM_ERR_INVALID_ARG, "bad argument");
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    for (int g = 0; g < 3; g++) {
+        double total = 0.0;
+        for (auto &pr : e->tev[g]) {
+            float t = 0.f;
+            if (cudaEventElapsedTime(&t, pr.first, pr.second) == cudaSuccess) total += t;
+            cudaEventDestroy(pr.first);
+            cudaEventDestroy(pr.second);
+        }
+        e->tev[g].clear();
+        ms[g] = total;
+        launches[g] = e->tlaunch[g];
+        e->tlaunch[g] = 0;
+    }
+    return DDM_OK;
+}
+
+extern "C" int ddm_build_masks(int scale, const float *lambdas, int Q, float tol, unsigned char *mask,
+                               int *counts) {
+    clear_error();
+    if (scale < 2 || (scale & (scale - 1)) || !lambdas || Q <= 0 || !counts)
+        return fail(DDM_ERR_INVALID_ARG, "ddm_build_masks: bad argument");
+    std::vector<int> qp, idx, cnt;
+    build_masks(scale, std::vector<float>(lambdas, lambdas + Q), tol, &qp, &idx, &cnt);
+    std::copy(cnt.begin(), cnt.end(), counts);
+    if (mask) {
+        const long long n = static_cast<long long>(scale) * (scale / 2 + 1);
+        std::memset(mask, 0, static_cast<size_t>(n * Q));
+        for (int q = 0; q < Q; q++)
+            for (int i = qp[q]; i < qp[q + 1]; i++) mask[q * n + idx[i]] = 1;
+    }
+    return DDM_OK;
+}
+
+extern "C" int ddm_compat_schedule(int N, int C, int multistream, int G, const int *taus, int T, int max_calls,
+                                   int *a_out, int *b_out, int *epoch_out, int *frames_read) {
+    clear_error();
+    if (N < 0 || C <= 0 || !taus || T <= 0 || !a_out || !b_out)
+        return fail(DDM_ERR_INVALID_ARG, "ddm_compat_schedule: bad argument");
+    std::vector<int> t(taus, taus + T);
+    for (int v : t)
+        if (v < 0 || v > C) return fail(DDM_ERR_INVALID_ARG, "taus must lie in [0, chunk]");
+    int fr = 0;
+    std::vector<CompatIteration> its = compat_schedule(N, C, multistream, G, t, &fr);
+    long long calls = 0;
+    for (const CompatIteration &it : its) calls += it.count;
+    if (calls > max_calls) return -1;
+    int c = 0, ep = 0;
+    for (const CompatIteration &it : its) {
+        for (int fo = 0; fo < it.count; fo++, c++) {
+            a_out[c] = it.start[fo];
+            for (int i = 0; i < T; i++) {
+                const int p = fo + t[i];
+                b_out[static_cast<long long>(c) * T + i] = p < C ? it.start[p] : it.end[p - C];
+            }
+            if (epoch_out) epoch_out[c] = ep;
+        }
+        if (it.dump_after) ep++;
+    }
+    if (frames_read) *frames_read = fr;
+    return c;
+}
+
+extern "C" void *ddm_host_alloc(size_t bytes) {
+    void *p = nullptr;
+    if (cudaMallocHost(&p, bytes) != cudaSuccess) {
+        fail(DDM_ERR_OUT_OF_MEMORY, "cudaMallocHost of " + std::to_string(bytes) + " bytes failed");
+        return nullptr;
+    }
+    return p;
+}
+
+extern "C" void ddm_host_free(void *p) {
+    if (p) cudaFreeHost(p);
+}
+
+extern "C" const char *ddm_status_string(int status) {
+    switch (status) {
+        case DDM_OK: return "ok";
+        case DDM_ERR_INVALID_ARG: return "invalid argument";
+        case DDM_ERR_CUDA: return "CUDA error";
+        case DDM_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case DDM_ERR_STATE: return "invalid state";
+        case DDM_ERR_NEED_FRAMES: return "frames missing";
+        case DDM_ERR_NO_DEVICE: return "no suitable CUDA device";
+        case DDM_ERR_IO: return "I/O error";
+        default: return "unknown status";
+    }
+}
+
+extern "C" int ddm_write_isf_file(const char *path, const double *isf_qt, const float *lambdas, int Q,
+                                  const int *taus, int T, float fps) {
+    clear_error();
+    if (!path || !isf_qt || !lambdas || !taus || Q <= 0 || T <= 0)
+        return fail(DDM_ERR_INVALID_ARG, "ddm_write_isf_file: bad argument");
+    std::vector<float> l(lambdas, lambdas + Q);
+    std::vector<int> t(taus, taus + T);
+    if (!write_isf_file(path, isf_qt, l, t, fps))
+        return fail(DDM_ERR_IO, std::string("[Out Error] Unable to open ") + path + ".");
+    return DDM_OK;
+}

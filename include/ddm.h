@@ -1,0 +1,216 @@
+/*
+ * ddm.h -- C ABI of the B200 multi-scale DDM engine (libddm_b200.so).
+ *
+ * The engine computes the image structure function D(q, tau) of a video at several
+ * tile scales at once: every frame's square region of interest (side M = largest
+ * scale) is cut into (M/s)^2 tiles per scale s, each tile gets a 2-D R2C FFT, the
+ * spectra of the last frames stay in a device-resident ring, |F(t+tau) - F(t)|^2 is
+ * accumulated per (tau, tile, k), and a masked azimuthal average over the annulus
+ * |k| in [q, tol*q] (q = s/lambda) turns each (scale, tile) into ISF[lambda][tau].
+ *
+ * The reference program (zhangyuyi99/cuda_multiDDM) has no library API: everything
+ * lives in one 24-argument function, runDDM (src/DDM.cu:268-292), driven by the ./ddm
+ * command line (src/main.cpp). Each entry point below names the part of that program
+ * it replaces. All calls return a ddm_status (0 = success) instead of exiting the
+ * process (src/debug.cpp:10-15,33-45). The engine owns all device memory it
+ * allocates; the caller owns every host buffer and every device buffer it passes in.
+ * One engine is used from one host thread at a time.
+ */
+#ifndef DDM_B200_H
+#define DDM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    DDM_OK = 0,
+    DDM_ERR_INVALID_ARG = 1,   /* a parameter is out of range; see ddm_last_error() */
+    DDM_ERR_CUDA = 2,          /* a CUDA runtime call failed */
+    DDM_ERR_OUT_OF_MEMORY = 3, /* device allocation failed or the HBM budget is exceeded */
+    DDM_ERR_STATE = 4,         /* call not valid in the engine's current state */
+    DDM_ERR_NEED_FRAMES = 5,   /* finalize needs frames that were never submitted */
+    DDM_ERR_NO_DEVICE = 6,     /* no CUDA device, or not an sm_100 device */
+    DDM_ERR_IO = 7             /* file could not be read or written */
+} ddm_status;
+
+/* How a source pixel becomes the FFT input value. */
+typedef enum {
+    DDM_PIX_BYTE0 = 0, /* first byte of each bytes_per_pixel-byte pixel: what the reference
+                          does for every input, 16-bit included (src/DDM_kernel.cuh:74-75) */
+    DDM_PIX_U16LE = 1  /* full little-endian 16-bit value (bytes_per_pixel must be 2) */
+} ddm_pixel_mode;
+
+/* Which frame pairs enter the accumulators and how each tau is normalised. */
+typedef enum {
+    DDM_EST_COMPAT = 0,  /* the reference's own schedule (src/DDM.cu:750-843), including which
+                            frame each tail frame pairs with, normalised by N (src/DDM.cu:875);
+                            needs total_frames and tau_max <= chunk_frames */
+    DDM_EST_UNBIASED = 1 /* every pair (t, t+tau) with t + tau < frames seen, normalised by the
+                            number of such pairs; no limit on tau_max */
+} ddm_estimator;
+
+typedef struct {
+    int frame_width, frame_height; /* source frame size in pixels */
+    int bytes_per_pixel;           /* 1 or 2 (also the channel stride for DDM_PIX_BYTE0) */
+    int pixel_mode;                /* ddm_pixel_mode */
+    int x_offset, y_offset;        /* ROI origin in the source frame (-x, -y) */
+    const int *scales;             /* tile sides, powers of two (any order; sorted descending) */
+    int scale_count;
+    const int *taus;               /* lags in frames (any order; sorted ascending) */
+    int tau_count;
+    const float *lambdas;          /* wavelengths in pixels (any order; sorted ascending) */
+    int lambda_count;
+    float tolerance;               /* annulus outer radius / inner radius (reference default 1.2f) */
+    int chunk_frames;              /* C: frames per ingest step (-C) */
+    int estimator;                 /* ddm_estimator */
+    int multistream;               /* compat only: 1 = reference default, 0 = its -Z schedule */
+    int total_frames;              /* N (-N); required for DDM_EST_COMPAT, 0 = open-ended */
+    int dump_every;                /* G (-G): ISF snapshot + accumulator purge every G chunks */
+    size_t hbm_budget_bytes;       /* refuse to open if the engine would need more; 0 = no limit */
+    int device;                    /* CUDA device ordinal */
+    void *stream;                  /* cudaStream_t to run on; NULL = the engine creates one */
+} ddm_config;
+
+typedef struct ddm_engine ddm_engine;
+
+/* Validation, allocation, mask construction and ring set-up: replaces the first half of
+ * runDDM (src/DDM.cu:301-744: sort + checks :319-355,459-463, buffers :493-641, cuFFT
+ * plans :648-677, ring pointers :686-742) and buildAzimuthMask (src/azimuthal_average.cu:229).
+ * Arrays in cfg are copied. */
+int ddm_open(const ddm_config *cfg, ddm_engine **out);
+
+/* Release every device and host resource of the engine. */
+int ddm_close(ddm_engine *e);
+
+/* Submit `count` consecutive source frames, each frame_height rows of
+ * frame_width*bytes_per_pixel bytes, rows packed. `on_device` = 0: host memory (pinned
+ * memory gives asynchronous copies); 1: device memory on the engine's device, read in
+ * place. Frames are transformed into the ring and every lag pair that becomes complete
+ * is accumulated. Replaces the chunk loop of runDDM (src/DDM.cu:765-843: H2D copy :767,
+ * parseChunk :154 -> parseBufferScalePow2 + cufftExecR2C, analyseChunk :222 ->
+ * processFFT). Returns once the work is queued on the engine's stream. */
+int ddm_submit_frames(ddm_engine *e, const void *frames, int count, int on_device);
+
+/* Queue the remaining pairs (compat tail, src/DDM.cu:830-843) and the masked azimuthal
+ * average of every (scale, tile, lambda, tau) bin; the result is ready for
+ * ddm_read_isf. Replaces combineAccumulators + analyse_accums + analyseFFTDevice
+ * (src/DDM.cu:45-63,72-146,864-876; src/azimuthal_average.cu:292-346). */
+int ddm_finalize(ddm_engine *e);
+
+/* Number of doubles in one ISF result: sum over scales of tiles * lambda_count * tau_count. */
+long ddm_isf_size(const ddm_engine *e);
+
+/* Copy the finalized ISF, layout [scale (descending)][tile][lambda (ascending)][tau
+ * (ascending)], into host memory (waits for the engine's stream). */
+int ddm_read_isf(ddm_engine *e, double *isf_out, long capacity);
+
+/* -G snapshots (src/DDM.cu:800-826): number of snapshots taken so far, and a copy of
+ * snapshot `index` in the ddm_read_isf layout. */
+int ddm_dump_count(const ddm_engine *e);
+int ddm_read_dump(ddm_engine *e, int index, double *isf_out, long capacity);
+
+/* Zero the accumulators and pair counts (the -G purge, src/DDM.cu:815-823). */
+int ddm_reset_accumulators(ddm_engine *e);
+
+/* Block until all queued work is done; returns the first asynchronous error. */
+int ddm_synchronize(ddm_engine *e);
+
+/* Sorted parameter arrays as the engine uses them (the reference sorts the caller's
+ * arrays in place, src/DDM.cu:319-321; the engine leaves them alone and exposes the
+ * sorted copies here). Any pointer may be NULL. */
+int ddm_get_params(const ddm_engine *e, int *scales, int *taus, float *lambdas);
+
+/* Annulus pixel counts per (scale, lambda) as [scale][lambda] (the h_pixel_counts of
+ * buildAzimuthMask, src/azimuthal_average.cu:271), and the boolean mask of one scale as
+ * [lambda][ky][kx] bytes, kx in [0, s/2]. */
+int ddm_get_pixel_counts(const ddm_engine *e, int *counts_out);
+int ddm_get_mask(const ddm_engine *e, int scale_index, unsigned char *mask_out, long capacity);
+
+/* Spectrum of frame `frame` (0-based submission index, still in the ring) as interleaved
+ * complex float [scale][tile][ky][kx]; and the raw accumulators as [tau][element]
+ * (sum - compensation, unnormalised |dF|^2 sums), both for tests. */
+long ddm_frame_elements(const ddm_engine *e);
+int ddm_read_spectrum(ddm_engine *e, int frame, float *out, long capacity);
+int ddm_read_accumulators(ddm_engine *e, double *out, long capacity);
+
+/* Engine facts: frames submitted, ring slots, device bytes held, kernels launched so far,
+ * the stream the engine runs on (a cudaStream_t), and for DDM_EST_COMPAT the number of
+ * frames the reference schedule reads (max(N, 2C) when N < 2C, else N; 0 otherwise). */
+typedef struct {
+    long frames_submitted;
+    int ring_slots;
+    size_t device_bytes;
+    long kernel_launches;
+    void *stream;
+    long frames_needed;
+} ddm_info;
+int ddm_get_info(const ddm_engine *e, ddm_info *info);
+
+/* Kernel timing: when enabled, the engine brackets every kernel it launches with CUDA
+ * events on its stream. ddm_kernel_times waits for the stream, then returns for each
+ * group -- 0 the FFT passes (parseChunk + cufftExecR2C in the reference), 1 the lag
+ * kernel (processFFT), 2 the azimuthal reduction (analyseFFTDevice) -- the summed device
+ * milliseconds and the number of launches since the last call, and clears them. */
+int ddm_set_timing(ddm_engine *e, int enabled);
+int ddm_kernel_times(ddm_engine *e, double *ms_out, long *launches_out);
+
+/* Host-only helpers (no GPU needed). ddm_build_masks: the annulus masks of one scale,
+ * [lambda][ky][kx] bytes (kx in [0, s/2]; mask_out may be NULL) and per-lambda pixel
+ * counts, bit-exact to buildAzimuthMask with q = s/lambda (src/azimuthal_average.cu:229-283,
+ * src/DDM.cu:101-105). ddm_compat_schedule: the frame pairs of the reference's chunk loop
+ * (src/DDM.cu:750-843) -- for each analysed frame c in order, the A-frame label a_out[c]
+ * and the partner label of every tau b_out[c*tau_count + t] (labels count frames from the
+ * first one read; -1 = device memory the reference never wrote), epoch_out[c] = -G purges
+ * before c (may be NULL); returns the number of analysed frames, or -1 if max_calls is too
+ * small; *frames_read = frames the reference reads from its source. */
+int ddm_build_masks(int scale, const float *lambdas, int lambda_count, float tolerance,
+                    unsigned char *mask_out, int *counts_out);
+int ddm_compat_schedule(int total_frames, int chunk, int multistream, int dump_every, const int *taus,
+                        int tau_count, int max_calls, int *a_out, int *b_out, int *epoch_out,
+                        int *frames_read);
+
+/* Page-locked host memory for frame buffers (asynchronous copies); NULL on failure. */
+void *ddm_host_alloc(size_t bytes);
+void ddm_host_free(void *ptr);
+
+/* Text of the last error on this thread. */
+const char *ddm_last_error(void);
+const char *ddm_status_string(int status);
+
+/* One (scale, tile) ISF text file, byte-compatible with writeIqtToFile
+ * (src/azimuthal_average.cu:112-150): line 1 the lambdas, line 2 tau/fps with the frame
+ * rate truncated to an integer as the reference does (src/DDM.cu:79,876), then one line
+ * of tau values per lambda; every value %g with a trailing space. */
+int ddm_write_isf_file(const char *path, const double *isf_qt, const float *lambdas,
+                       int lambda_count, const int *taus, int tau_count, float fps);
+
+/* Seeded synthetic Brownian-particle video (host memory, frame-major): background +
+ * Gaussian spots of peak `amplitude` and width `spot_sigma`, positions uniform, each
+ * frame every spot steps N(0, step_var) per axis (step_var_b for the second half of the
+ * spots), periodic boundaries; then additive Gaussian noise of sd `noise_sd`
+ * (noise_sd < 0: Poisson shot noise), rounded half-to-even and clipped to [0, max_value].
+ * Pixels are 1 byte if max_value <= 255, else 2 bytes little-endian. */
+int ddm_synth_video(uint64_t seed, int width, int height, int frames, int spots,
+                    double spot_sigma, double amplitude, double background, double step_var,
+                    double step_var_b, double noise_sd, int max_value, void *out);
+
+/* Camera .movie files (src/video_reader.cpp:64-290): open, describe, read frames. */
+typedef struct {
+    int width, height, bytes_per_pixel;
+    float fps;               /* 1e6 / (timestamp[1] - timestamp[0]), as the reference */
+    int camera_type;         /* 1 IIDC, 2 Andor, 3 Ximea */
+    int pixel_mode;          /* 1 mono8, 2 mono16 big-endian, 3 mono16 little-endian */
+} ddm_movie_info;
+typedef struct ddm_movie ddm_movie;
+int ddm_movie_open(const char *path, int frame_offset, ddm_movie **out, ddm_movie_info *info);
+int ddm_movie_read(ddm_movie *m, void *dst, int count); /* frames packed, w*h*bpp each */
+int ddm_movie_close(ddm_movie *m);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,182 @@
+"""GPU parity tests: the CUDA engine (through the C ABI) against the FP64 oracle.
+
+Tolerance: ISF values agree with the FP64 oracle to 1e-5 relative per bin (FP32 FFT and
+lag arithmetic; FP64 azimuthal reduction), with an absolute floor of 1e-9 of the largest
+value of the (scale, tile) block for bins that are exactly zero in FP64.
+"""
+import numpy as np
+import pytest
+
+from cuda_multiddm_b200 import DDMError, Engine, EngineConfig, media
+from cuda_multiddm_b200._lib import lib
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-5
+
+
+def assert_isf_close(got, want, scales, Q, T, rtol=RTOL):
+    off = 0
+    worst = 0.0
+    ss = sorted(scales, reverse=True)
+    for s in ss:
+        size = (ss[0] // s) ** 2 * Q * T
+        g, w = got[off:off + size], want[off:off + size]
+        floor = 1e-9 * max(np.abs(w).max(), 1e-300)
+        err = np.abs(g - w) / np.maximum(np.abs(w), floor)
+        worst = max(worst, float(err.max()))
+        assert np.all(np.abs(g - w) <= rtol * np.abs(w) + floor), (s, float(err.max()))
+        off += size
+    return worst
+
+
+def engine_run(frames, scales, taus, lambdas, *, estimator, N=None, C=10, tol=1.2, multistream=True, G=0,
+               x_off=0, y_off=0, pixel_mode="byte0", on_device=False):
+    n, h, w = frames.shape[:3]
+    bpp = 2 if frames.dtype == np.uint16 else 1
+    raw = np.ascontiguousarray(frames).view(np.uint8).reshape(n, h, w * bpp)
+    N = n if N is None else N
+    cfg = EngineConfig(frame_width=w, frame_height=h, scales=scales, taus=taus, lambdas=lambdas, tolerance=tol,
+                       chunk_frames=C, estimator=estimator, total_frames=N, multistream=multistream, dump_every=G,
+                       bytes_per_pixel=bpp, pixel_mode=pixel_mode, x_offset=x_off, y_offset=y_off)
+    with Engine(cfg) as eng:
+        need = eng.info().frames_needed if estimator == "compat" else N
+        if on_device:
+            import torch
+            t = torch.from_numpy(raw[:need].copy()).cuda()
+            eng.submit(t)
+            torch.cuda.synchronize()
+        else:
+            eng.submit(raw[:need])
+        eng.finalize()
+        return eng.isf(), eng.dumps(), eng.info()
+
+
+@pytest.mark.parametrize("M,scales", [(256, [256, 128, 64, 32, 16, 8, 4, 2]), (2048, [2048, 1024])])
+def test_spectra_match_fp64_fft(M, scales):
+    rng = np.random.default_rng(M)
+    frames = rng.integers(0, 256, size=(3, M, M), dtype=np.uint8)
+    cfg = EngineConfig(frame_width=M, frame_height=M, scales=scales, taus=[1], lambdas=[2.0], chunk_frames=4)
+    with Engine(cfg) as eng:
+        eng.submit(frames)
+        spec = eng.spectrum(1)
+    off = 0
+    for s in sorted(scales, reverse=True):
+        tiles_side = M // s
+        ref_tiles = O.extract(frames[1], 1, 0, 0, 0, M, s)
+        for tile in [0, tiles_side * tiles_side - 1, (tiles_side * tiles_side) // 2]:
+            ref = O.fft2_r2c(ref_tiles[tile])
+            n = s * (s // 2 + 1)
+            got = spec[off + tile * n: off + (tile + 1) * n].reshape(s, s // 2 + 1)
+            scale = np.abs(ref).max()
+            assert np.abs(got - ref).max() <= 2e-6 * scale, (s, tile)
+            assert np.linalg.norm(got - ref) <= 1e-6 * np.linalg.norm(ref), (s, tile)
+        off += tiles_side * tiles_side * s * (s // 2 + 1)
+
+
+def _golden_cases():
+    from cases import CASES
+    return CASES
+
+
+@pytest.mark.parametrize("case", _golden_cases(), ids=lambda c: c.name)
+def test_compat_matches_oracle(case):
+    frames = case.frames()
+    if case.frame_offset:
+        frames = frames[case.frame_offset:]
+    kw = dict(estimator="compat", N=case.N, C=case.C, tol=case.tolerance, multistream=case.multistream,
+              G=case.dump_every, x_off=case.x_off, y_off=case.y_off)
+    isf, dumps, _ = engine_run(frames, case.scales, case.taus, case.lambdas, **kw)
+    want, want_dumps = O.ddm_run(frames, case.scales, case.taus, case.lambdas, tol=case.tolerance, N=case.N,
+                                 chunk=case.C, multistream=case.multistream, estimator=O.EST_COMPAT,
+                                 dump_every=case.dump_every, x_off=case.x_off, y_off=case.y_off)
+    Q, T = len(case.lambdas), len(case.taus)
+    assert_isf_close(isf, want, case.scales, Q, T)
+    assert len(dumps) == len(want_dumps)
+    for d, wd in zip(dumps, want_dumps):
+        assert_isf_close(d, wd, case.scales, Q, T)
+
+
+def test_unbiased_multiscale_matches_oracle():
+    frames = media.synth_video(77, 256, 256, 80, 150, step_var=1.0)
+    scales = [256, 128, 64, 32]
+    taus = [1, 2, 3, 5, 8, 13, 21, 34, 55]   # tau_max > chunk: only the unbiased path allows it
+    lambdas = [2.0, 3.5, 6.0, 10.0, 17.0, 29.0, 50.0]
+    isf, _, info = engine_run(frames, scales, taus, lambdas, estimator="unbiased", C=10)
+    want, _ = O.ddm_run(frames, scales, taus, lambdas, estimator=O.EST_UNBIASED, chunk=10)
+    assert_isf_close(isf, want, scales, len(lambdas), len(taus))
+    assert info.ring_slots == 55 + 10
+
+
+def test_u16_full_precision_matches_oracle():
+    frames = media.synth_video(15, 64, 64, 24, 30, amplitude=2000, background=300, noise_sd=-1, max_value=4095)
+    isf, _, _ = engine_run(frames, [64, 32], [1, 2, 4], [4.0, 8.0, 16.0], estimator="unbiased", C=8,
+                           pixel_mode="u16")
+    want, _ = O.ddm_run(frames, [64, 32], [1, 2, 4], [4.0, 8.0, 16.0], estimator=O.EST_UNBIASED, chunk=8,
+                        pixmode=O.PIX_U16LE)
+    assert_isf_close(isf, want, [64, 32], 3, 3)
+
+
+def test_device_and_host_submission_identical():
+    frames = media.synth_video(9, 160, 144, 30, 60)
+    args = ([128, 64], [1, 2, 5, 11], [2.0, 5.0, 9.0, 20.0])
+    kw = dict(estimator="unbiased", C=7, x_off=20, y_off=9)
+    a, _, _ = engine_run(frames, *args, **kw)
+    b, _, _ = engine_run(frames, *args, on_device=True, **kw)
+    assert np.array_equal(a, b)
+
+
+def test_static_video_is_zero_and_intensity_scales_quadratically():
+    static = np.repeat(media.synth_video(4, 64, 64, 1, 20, noise_sd=0.0), 12, axis=0)
+    isf, _, _ = engine_run(static, [64, 32], [1, 3], [4.0, 8.0], estimator="unbiased", C=4)
+    assert np.all(isf == 0.0)
+    base = media.synth_video(5, 64, 64, 20, 20, amplitude=50, background=10, noise_sd=2.0, max_value=120)
+    i1, _, _ = engine_run(base, [64], [1, 2, 3], [4.0, 8.0, 16.0], estimator="unbiased", C=5)
+    i2, _, _ = engine_run((base.astype(np.uint16) * 2).astype(np.uint8), [64], [1, 2, 3], [4.0, 8.0, 16.0],
+                          estimator="unbiased", C=5)
+    np.testing.assert_allclose(i2, 4.0 * i1, rtol=1e-5)
+
+
+def test_chunking_does_not_change_unbiased_result():
+    frames = media.synth_video(21, 64, 64, 45, 30)
+    args = ([64, 32], [1, 2, 4, 9, 17], [3.0, 6.0, 12.0])
+    a, _, _ = engine_run(frames, *args, estimator="unbiased", C=5)
+    b, _, _ = engine_run(frames, *args, estimator="unbiased", C=32)
+    assert_isf_close(a, b, [64, 32], 3, 5, rtol=2e-6)
+
+
+def test_errors_are_status_codes():
+    base = dict(frame_width=64, frame_height=64, taus=[1, 2], lambdas=[4.0], chunk_frames=4)
+    with pytest.raises(DDMError) as e:
+        Engine(EngineConfig(scales=[48], **base))
+    assert "powers of two" in str(e.value)
+    with pytest.raises(DDMError) as e:
+        Engine(EngineConfig(scales=[128], **base))
+    assert "smaller than actual image size" in str(e.value)
+    with pytest.raises(DDMError) as e:
+        Engine(EngineConfig(scales=[64], estimator="compat", total_frames=8, **{**base, "taus": [1, 9]}))
+    assert "largest tau value" in str(e.value)
+    with pytest.raises(DDMError) as e:
+        Engine(EngineConfig(scales=[64], hbm_budget_bytes=1000, **base))
+    assert e.value.status == 3
+    with pytest.raises(DDMError) as e:
+        Engine(EngineConfig(scales=[64], estimator="compat", total_frames=8,
+                            **{**base, "lambdas": [100.0]}))
+    assert "smallest scale" in str(e.value)
+    # compat: frames beyond what the reference reads are refused; finalize without frames fails
+    cfg = EngineConfig(scales=[64], estimator="compat", total_frames=8, **base)
+    with Engine(cfg) as eng:
+        with pytest.raises(DDMError) as e:
+            eng.finalize()
+        assert e.value.status == 5
+        with pytest.raises(DDMError):
+            eng.submit(np.zeros((9, 64, 64), np.uint8))
+
+
+def test_kernel_launches_counted():
+    frames = media.synth_video(2, 64, 64, 8, 10)
+    _, _, info = engine_run(frames, [64, 32], [1, 2], [4.0], estimator="unbiased", C=4)
+    # per piece of 4 frames: 2 FFT passes per scale + 1 lag launch; 1 azimuthal launch
+    assert info.kernel_launches == 2 * (2 * 2 + 1) + 1
+    assert lib() is not None
