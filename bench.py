@@ -44,6 +44,9 @@ SCALES = [1024, 512, 256, 128]
 CHUNK = 30
 N_FRAMES = 1000
 SIDE = 1024
+# A 4x smaller frame with the same tau list and chunk (the same lag schedule per element),
+# small enough for ncu captures that save and restore device memory (about 3 GB held).
+SMALL = dict(SIDE=512, SCALES=[512, 256, 128, 64], N_FRAMES=300)
 
 
 def workload():
@@ -60,10 +63,11 @@ def lag_bytes_per_frame(T: int) -> float:
     return 8.0 * E * (T + 1) + 16.0 * T * E / CHUNK
 
 
-def make_video(seed: int, frames: int = N_FRAMES) -> np.ndarray:
+def make_video(seed: int, frames: int | None = None) -> np.ndarray:
     from cuda_multiddm_b200.media import synth_video
-    return synth_video(seed, SIDE, SIDE, frames, 4000, spot_sigma=2.0, amplitude=120.0, background=20.0,
-                       step_var=2.0, noise_sd=4.0, max_value=255)
+    spots = 4000 * SIDE * SIDE // (1024 * 1024)  # same spot density at every frame size
+    return synth_video(seed, SIDE, SIDE, N_FRAMES if frames is None else frames, spots, spot_sigma=2.0,
+                       amplitude=120.0, background=20.0, step_var=2.0, noise_sd=4.0, max_value=255)
 
 
 def measured_peaks():
@@ -280,7 +284,8 @@ def run_ours(args) -> None:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "multiscale_1024_4scales_64tau", "frames": N_FRAMES, "side": SIDE,
+                "config": {"workload": "multiscale_1024_4scales_64tau" if SIDE == 1024 else
+                           "small_512_4scales_64tau (profiling)", "frames": N_FRAMES, "side": SIDE,
                            "scales": SCALES, "taus": T, "tau_max": max(taus), "lambdas": len(lambdas),
                            "chunk": CHUNK, "estimator": "unbiased", "steady_state": True,
                            "l2": "inputs larger than L2 (ring of %d frames x %.1f MB)"
@@ -310,7 +315,11 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["multiscale", "small"], default="multiscale",
+                    help="small: 512^2 frames, scales 512..64, same taus and chunk (profiling only)")
     args = ap.parse_args()
+    if args.workload == "small":
+        globals().update(SMALL)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <string>
 #include <vector>
 
@@ -22,6 +23,7 @@
 #include "errors.hpp"
 #include "host.hpp"
 #include "kernels.cuh"
+#include "lag.cuh"
 
 namespace ddm {
 
@@ -82,6 +84,7 @@ struct ddm_engine {
     int tab_stride = 0, tab_next = 0;
     int *q_ptr_d = nullptr, *idx_d = nullptr, *counts_d = nullptr;
     double *norm_d = nullptr, *isf_d = nullptr;
+    int *status_d = nullptr;                // set by kernels whose bounded waits ran out
     size_t device_bytes = 0;
     std::vector<int> counts_h;             // [S][Q]
     std::vector<std::vector<int>> q_ptr_s, idx_s;  // per scale CSR (host copy)
@@ -135,6 +138,7 @@ void free_all(ddm_engine *e) {
     cudaFree(e->counts_d);
     cudaFree(e->norm_d);
     cudaFree(e->isf_d);
+    cudaFree(e->status_d);
     if (e->tables_h) cudaFreeHost(e->tables_h);
     for (int i = 0; i < kTables; i++)
         if (e->tab_ev[i]) cudaEventDestroy(e->tab_ev[i]);
@@ -232,11 +236,25 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
 // Lag launches
 // ---------------------------------------------------------------------------------
 
+// Entries must come with ascending window starts (ent_w). The windows of all entries
+// are merged into the sorted list of distinct partner positions (the union); entry e's
+// window is then union indices [ub_e, ub_e + nreg), always the tail of the list at the
+// time the entry is appended, because windows are contiguous and start in order.
 int launch_lag(ddm_engine *e, const Launch &L) {
     if (L.nreg <= 0 || L.ent_acc.empty()) return DDM_OK;
     const int ntau = static_cast<int>(L.ent_acc.size());
-    const int npos = static_cast<int>(L.pos.size());
-    const int ntab = kTabEntries + 2 * ntau + npos;
+    std::vector<int> ub(ntau), uslot;
+    uslot.reserve(L.pos.size());
+    int next = std::numeric_limits<int>::min();  // first position past the union so far
+    for (int i = 0; i < ntau; i++) {
+        const int w = L.ent_w[i];
+        if (i > 0 && w <= L.ent_w[i - 1]) return fail(DDM_ERR_STATE, "internal: lag windows out of order");
+        for (int p = std::max(w, next); p < w + L.nreg; p++) uslot.push_back(L.pos[p]);
+        next = std::max(next, w + L.nreg);
+        ub[i] = static_cast<int>(uslot.size()) - L.nreg;
+    }
+    const int nu = static_cast<int>(uslot.size());
+    const int ntab = kTabEntries + 2 * ntau + nu;
     if (ntab > e->tab_stride) return fail(DDM_ERR_STATE, "internal: lag table overflow");
     const int ts = e->tab_next;
     e->tab_next = (e->tab_next + 1) % kTables;
@@ -244,28 +262,38 @@ int launch_lag(ddm_engine *e, const Launch &L) {
     int *th = e->tables_h + static_cast<size_t>(ts) * e->tab_stride;
     th[kTabNreg] = L.nreg;
     th[kTabNtau] = ntau;
-    th[kTabNpos] = npos;
+    th[kTabNunion] = nu;
     for (int j = 0; j < kMaxJ; j++) th[kTabReg + j] = j < L.nreg ? L.reg[j] : -1;
     std::copy(L.ent_acc.begin(), L.ent_acc.end(), th + kTabEntries);
-    std::copy(L.ent_w.begin(), L.ent_w.end(), th + kTabEntries + ntau);
-    std::copy(L.pos.begin(), L.pos.end(), th + kTabEntries + 2 * ntau);
+    std::copy(ub.begin(), ub.end(), th + kTabEntries + ntau);
+    std::copy(uslot.begin(), uslot.end(), th + kTabEntries + 2 * ntau);
     int *td = e->tables_d + static_cast<size_t>(ts) * e->tab_stride;
     CUDA_TRY(cudaMemcpyAsync(td, th, sizeof(int) * ntab, cudaMemcpyHostToDevice, e->stream));
     CUDA_TRY(cudaEventRecord(e->tab_ev[ts], e->stream));
     e->tab_used[ts] = true;
 
-    const unsigned blocks = static_cast<unsigned>((e->E + kLagThreads - 1) / kLagThreads);
-    const size_t smem = sizeof(int) * ntab;
+    const unsigned blocks = static_cast<unsigned>((e->E + kLagBlock - 1) / kLagBlock);
+    const size_t smem = lag_smem_bytes(ntab);
     TimedRange tr(e, 1);
     if (L.nreg <= 8)
-        lag_kernel<8><<<blocks, kLagThreads, smem, e->stream>>>(e->ring, e->acc, e->E, td);
+        lag_pipe_kernel<8><<<blocks, kLagBlock, smem, e->stream>>>(e->ring, e->acc, e->E, td, e->status_d);
     else if (L.nreg <= 16)
-        lag_kernel<16><<<blocks, kLagThreads, smem, e->stream>>>(e->ring, e->acc, e->E, td);
+        lag_pipe_kernel<16><<<blocks, kLagBlock, smem, e->stream>>>(e->ring, e->acc, e->E, td, e->status_d);
     else
-        lag_kernel<32><<<blocks, kLagThreads, smem, e->stream>>>(e->ring, e->acc, e->E, td);
+        lag_pipe_kernel<32><<<blocks, kLagBlock, smem, e->stream>>>(e->ring, e->acc, e->E, td, e->status_d);
     CUDA_TRY(cudaGetLastError());
     tr.end(1);
     e->launches++;
+    return DDM_OK;
+}
+
+// Device status word set by kernels whose bounded waits ran out.
+int check_device_status(ddm_engine *e) {
+    int st = 0;
+    CUDA_TRY(cudaMemcpyAsync(&st, e->status_d, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    if (st != 0) return fail(DDM_ERR_CUDA, "a lag-kernel pipeline wait timed out (device status " +
+                                               std::to_string(st) + "); results are incomplete");
     return DDM_OK;
 }
 
@@ -455,8 +483,9 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
     e->T = static_cast<int>(e->taus.size());
     e->Q = static_cast<int>(e->lambdas.size());
     e->tau_max = e->taus.back();
-    if (e->tau_max > 40000 || e->T > 8192)
-        return bail(fail(DDM_ERR_INVALID_ARG, "tau_max must be <= 40000 and at most 8192 taus"));
+    if (lag_smem_bytes(kTabEntries + 2 * e->T + kMaxJ + e->tau_max) > static_cast<size_t>(kLagSmemMax))
+        return bail(fail(DDM_ERR_INVALID_ARG, "tau list too long: 2 * tau_count + tau_max must stay below " +
+                                                  std::to_string((kLagSmemMax - lag_smem_bytes(kTabEntries + kMaxJ)) / 4)));
 
     // Geometry
     long long off = 0, isf_off = 0;
@@ -531,6 +560,8 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
     if ((st = dev_alloc(e, &e->tables_d, static_cast<size_t>(kTables) * e->tab_stride))) return bail(st);
     if ((st = dev_alloc(e, &e->norm_d, e->T))) return bail(st);
     if ((st = dev_alloc(e, &e->isf_d, e->isf_size))) return bail(st);
+    if ((st = dev_alloc(e, &e->status_d, 1))) return bail(st);
+    if (cudaMemset(e->status_d, 0, sizeof(int)) != cudaSuccess) return bail(fail(DDM_ERR_CUDA, "status memset failed"));
     if (cudaMallocHost(reinterpret_cast<void **>(&e->tables_h),
                        sizeof(int) * static_cast<size_t>(kTables) * e->tab_stride) != cudaSuccess)
         return bail(fail(DDM_ERR_OUT_OF_MEMORY, "pinned table buffer"));
@@ -576,12 +607,10 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
     // Kernel shared-memory limits (the FFT passes use up to 128 KB)
     if (cudaFuncSetAttribute(fft_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024) != cudaSuccess ||
         cudaFuncSetAttribute(fft_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024) != cudaSuccess ||
-        cudaFuncSetAttribute(lag_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess ||
-        cudaFuncSetAttribute(lag_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess ||
-        cudaFuncSetAttribute(lag_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
+        cudaFuncSetAttribute(lag_pipe_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
+        cudaFuncSetAttribute(lag_pipe_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
+        cudaFuncSetAttribute(lag_pipe_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess)
         return bail(fail(DDM_ERR_CUDA, "cudaFuncSetAttribute failed"));
-    if (sizeof(int) * e->tab_stride > 200 * 1024)
-        return bail(fail(DDM_ERR_INVALID_ARG, "tau list too long for the lag table"));
 
     if (cudaMemsetAsync(e->acc, 0, acc_bytes, e->stream) != cudaSuccess ||
         cudaMemsetAsync(e->ring, 0, ring_bytes, e->stream) != cudaSuccess ||
@@ -662,6 +691,7 @@ extern "C" int ddm_finalize(ddm_engine *e) {
         norm = e->pair_count;
     }
     if ((st = run_azimuth(e, norm))) return st;
+    if ((st = check_device_status(e))) return st;
     e->finalized = true;
     return DDM_OK;
 }
@@ -698,7 +728,7 @@ extern "C" int ddm_synchronize(ddm_engine *e) {
     if (!e) return fail(DDM_ERR_INVALID_ARG, "null engine");
     CUDA_TRY(cudaStreamSynchronize(e->stream));
     CUDA_TRY(cudaGetLastError());
-    return DDM_OK;
+    return check_device_status(e);
 }
 
 extern "C" int ddm_get_params(const ddm_engine *e, int *scales, int *taus, float *lambdas) {

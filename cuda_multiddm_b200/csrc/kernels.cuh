@@ -4,9 +4,8 @@
 //                      (replaces parseBufferScalePow2 + the first half of cufftExecR2C,
 //                      src/DDM_kernel.cuh:43-78, src/DDM.cu:188-192)
 //   fft_cols_kernel    column pass, in place in the ring slot
-//   lag_kernel         |F(a) - F(b)|^2 accumulation for a block of frames against every
-//                      tau, Kahan-compensated per chunk (replaces processFFT,
-//                      src/DDM_kernel.cuh:85-101, launched S*T*C times per chunk there)
+//   lag_pipe_kernel    (lag.cuh) |F(a) - F(b)|^2 accumulation for a block of frames
+//                      against every tau (replaces processFFT, src/DDM_kernel.cuh:85-101)
 //   azimuth_kernel     masked azimuthal average of every (scale, tile, tau) row over the
 //                      annulus index lists, FP64 (replaces maskReduce + host sums,
 //                      src/azimuthal_average.cu:292-346)
@@ -22,10 +21,6 @@ constexpr int kFftThreads = 256;
 constexpr int kLagThreads = 256;
 constexpr int kAzThreads = 256;
 constexpr int kMaxJ = 32;  // frames held in registers by one lag-kernel thread
-
-// Lag table layout (ints): header, register frames, tau entries, window positions.
-constexpr int kTabNreg = 0, kTabNtau = 1, kTabNpos = 2, kTabReg = 3;
-constexpr int kTabEntries = kTabReg + kMaxJ;  // then ntau acc indices, ntau window starts, npos slots
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -151,56 +146,6 @@ __global__ void __launch_bounds__(kFftThreads) fft_cols_kernel(ColArgs a) {
     for (int i = threadIdx.x; i < s * P; i += blockDim.x) {
         const int ky = i / P, p = i - ky * P;
         if (p < ncols) base[(long long)ky * nx + p] = sm[bitrev(ky, a.log2s) * P + p];
-    }
-}
-
-// One thread per spectrum element k. Register frames r[j] (j < nreg) are ring slots
-// table[kTabReg + j]; entry e pairs r[j] with window position w_e + j, whose ring slot
-// is pos[w_e + j] (-1: no such frame, pair skipped). The J pair sums of one entry are
-// added in FP32, then folded into the (sum, compensation) accumulator of tau index
-// acc_e with one Kahan step.
-template <int J>
-__global__ void __launch_bounds__(kLagThreads) lag_kernel(const float2 *__restrict__ ring,
-                                                          float2 *__restrict__ acc, long long E,
-                                                          const int *__restrict__ table) {
-    extern __shared__ int tab[];
-    const int ntab = kTabEntries + 2 * table[kTabNtau] + table[kTabNpos];
-    for (int i = threadIdx.x; i < ntab; i += blockDim.x) tab[i] = table[i];
-    __syncthreads();
-    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= E) return;
-    const int nreg = tab[kTabNreg], ntau = tab[kTabNtau];
-    const int *ent_acc = tab + kTabEntries;
-    const int *ent_w = ent_acc + ntau;
-    const int *pos = ent_w + ntau;
-    float2 r[J];
-#pragma unroll
-    for (int j = 0; j < J; j++) {
-        const int slot = j < nreg ? tab[kTabReg + j] : -1;
-        r[j] = slot >= 0 ? __ldg(ring + slot * E + k) : make_float2(0.f, 0.f);
-    }
-    for (int e = 0; e < ntau; e++) {
-        const int w = ent_w[e];
-        float sum = 0.f;
-#pragma unroll
-        for (int j = 0; j < J; j++) {
-            if (j < nreg && tab[kTabReg + j] >= 0) {
-                const int slot = pos[w + j];
-                if (slot >= 0) {
-                    const float2 b = __ldg(ring + slot * E + k);
-                    const float dx = r[j].x - b.x, dy = r[j].y - b.y;
-                    sum = fmaf(dx, dx, sum);
-                    sum = fmaf(dy, dy, sum);
-                }
-            }
-        }
-        float2 *ap = acc + (long long)ent_acc[e] * E + k;
-        float2 a = *ap;  // a.x running sum, a.y Kahan compensation
-        const float y = sum - a.y;
-        const float t = a.x + y;
-        a.y = (t - a.x) - y;
-        a.x = t;
-        *ap = a;
     }
 }
 
