@@ -57,6 +57,10 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
                  : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
     asm volatile(
         "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
@@ -114,13 +118,18 @@ __global__ void __launch_bounds__(kLagBlock, 2)
     const uint32_t bytes = static_cast<uint32_t>(
         sizeof(float2) * (E - e0 < kLagBlock ? E - e0 : static_cast<long long>(kLagBlock)));
 
-    // Producer state lives in thread 0 only.
+    // Producer state lives in thread 0 only. Union index u is the (u / kLagSlots)-th use of
+    // slot u % kLagSlots, and every use completes exactly one phase of the slot's barrier:
+    // a copy's transaction bytes, or a bare arrival when there is no frame to copy.
     int issued = 0;
     auto issue_upto = [&](int limit) {
         for (; issued < nu && issued < limit; issued++) {
             const int s = uslot[issued];
-            if (s < 0) continue;  // no such frame: nothing to copy, nobody waits
             uint64_t *bar = &full[issued % kLagSlots];
+            if (s < 0) {  // no such frame: nothing to copy, nobody waits; keep the phase count
+                mbar_arrive(bar);
+                continue;
+            }
             mbar_expect_tx(bar, bytes);
             bulk_load(slots + (issued % kLagSlots) * kLagBlock, ring + static_cast<long long>(s) * E + e0, bytes,
                       bar);
