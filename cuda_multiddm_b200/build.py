@@ -26,7 +26,6 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC,-fop
               f"-I{ROOT / 'include'}", f"-I{CSRC}"]
 
 SOURCES = ["engine.cu", "host.cpp", "synth.cpp", "movie.cpp"]
-HEADERS = ["kernels.cuh", "host.hpp", "errors.hpp"]
 
 
 def _nvcc() -> str:
@@ -53,7 +52,7 @@ def _run(cmd: list[str]) -> None:
 def build(force: bool = False, verbose: bool = False) -> Path:
     nvcc = _nvcc()
     BUILD.mkdir(exist_ok=True)
-    headers = [CSRC / h for h in HEADERS] + [ROOT / "include" / "ddm.h"]
+    headers = sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.hpp")) + [ROOT / "include" / "ddm.h"]
     objs = []
     for src in SOURCES:
         s = CSRC / src
