@@ -254,7 +254,20 @@ int launch_lag(ddm_engine *e, const Launch &L) {
         ub[i] = static_cast<int>(uslot.size()) - L.nreg;
     }
     const int nu = static_cast<int>(uslot.size());
-    const int ntab = kTabEntries + 2 * ntau + nu;
+    // Register-frame count the kernel is compiled for; entries whose whole window is present
+    // and that use all J register frames take the kernel's unchecked fast path.
+    int J = kLagJs[kNumLagJs - 1];
+    for (int i = kNumLagJs - 1; i >= 0; i--)
+        if (kLagJs[i] >= L.nreg) J = kLagJs[i];
+    bool regs_ok = L.nreg == J;
+    for (int j = 0; j < L.nreg; j++) regs_ok = regs_ok && L.reg[j] >= 0;
+    std::vector<int> full(ntau);
+    for (int i = 0; i < ntau; i++) {
+        bool f = regs_ok;
+        for (int j = 0; j < L.nreg && f; j++) f = uslot[ub[i] + j] >= 0;
+        full[i] = f ? 1 : 0;
+    }
+    const int ntab = kTabEntries + 3 * ntau + nu;
     if (ntab > e->tab_stride) return fail(DDM_ERR_STATE, "internal: lag table overflow");
     const int ts = e->tab_next;
     e->tab_next = (e->tab_next + 1) % kTables;
@@ -266,7 +279,8 @@ int launch_lag(ddm_engine *e, const Launch &L) {
     for (int j = 0; j < kMaxJ; j++) th[kTabReg + j] = j < L.nreg ? L.reg[j] : -1;
     std::copy(L.ent_acc.begin(), L.ent_acc.end(), th + kTabEntries);
     std::copy(ub.begin(), ub.end(), th + kTabEntries + ntau);
-    std::copy(uslot.begin(), uslot.end(), th + kTabEntries + 2 * ntau);
+    std::copy(full.begin(), full.end(), th + kTabEntries + 2 * ntau);
+    std::copy(uslot.begin(), uslot.end(), th + kTabEntries + 3 * ntau);
     int *td = e->tables_d + static_cast<size_t>(ts) * e->tab_stride;
     CUDA_TRY(cudaMemcpyAsync(td, th, sizeof(int) * ntab, cudaMemcpyHostToDevice, e->stream));
     CUDA_TRY(cudaEventRecord(e->tab_ev[ts], e->stream));
@@ -275,12 +289,13 @@ int launch_lag(ddm_engine *e, const Launch &L) {
     const unsigned blocks = static_cast<unsigned>((e->E + kLagBlock - 1) / kLagBlock);
     const size_t smem = lag_smem_bytes(ntab);
     TimedRange tr(e, 1);
-    if (L.nreg <= 8)
-        lag_pipe_kernel<8><<<blocks, kLagBlock, smem, e->stream>>>(e->ring, e->acc, e->E, td, e->status_d);
-    else if (L.nreg <= 16)
-        lag_pipe_kernel<16><<<blocks, kLagBlock, smem, e->stream>>>(e->ring, e->acc, e->E, td, e->status_d);
-    else
-        lag_pipe_kernel<32><<<blocks, kLagBlock, smem, e->stream>>>(e->ring, e->acc, e->E, td, e->status_d);
+    switch (J) {
+#define LAG_CASE(JJ) \
+    case JJ: lag_pipe_kernel<JJ><<<blocks, kLagBlock, smem, e->stream>>>(e->ring, e->acc, e->E, td, e->status_d); break;
+        LAG_CASE(4) LAG_CASE(8) LAG_CASE(16) LAG_CASE(20) LAG_CASE(24) LAG_CASE(30) LAG_CASE(32)
+#undef LAG_CASE
+        default: return fail(DDM_ERR_STATE, "internal: no lag kernel for this frame count");
+    }
     CUDA_TRY(cudaGetLastError());
     tr.end(1);
     e->launches++;
@@ -483,7 +498,7 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
     e->T = static_cast<int>(e->taus.size());
     e->Q = static_cast<int>(e->lambdas.size());
     e->tau_max = e->taus.back();
-    if (lag_smem_bytes(kTabEntries + 2 * e->T + kMaxJ + e->tau_max) > static_cast<size_t>(kLagSmemMax))
+    if (lag_smem_bytes(kTabEntries + 3 * e->T + kMaxJ + e->tau_max) > static_cast<size_t>(kLagSmemMax))
         return bail(fail(DDM_ERR_INVALID_ARG, "tau list too long: 2 * tau_count + tau_max must stay below " +
                                                   std::to_string((kLagSmemMax - lag_smem_bytes(kTabEntries + kMaxJ)) / 4)));
 
@@ -530,7 +545,7 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
     const size_t ring_bytes = sizeof(float2) * static_cast<size_t>(e->R) * e->E;
     const size_t acc_bytes = sizeof(float2) * static_cast<size_t>(e->T) * e->E;
     const size_t stage_bytes = static_cast<size_t>(e->jmax) * e->M * e->M * e->bpp;
-    e->tab_stride = kTabEntries + 2 * e->T + kMaxJ + e->tau_max + 4;
+    e->tab_stride = kTabEntries + 3 * e->T + kMaxJ + e->tau_max + 4;
     size_t need = ring_bytes + acc_bytes + stage_bytes + sizeof(double) * e->isf_size +
                   sizeof(int) * static_cast<size_t>(kTables) * e->tab_stride;
     if (cfg->hbm_budget_bytes && need > cfg->hbm_budget_bytes)
@@ -607,8 +622,12 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
     // Kernel shared-memory limits (the FFT passes use up to 128 KB)
     if (cudaFuncSetAttribute(fft_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024) != cudaSuccess ||
         cudaFuncSetAttribute(fft_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024) != cudaSuccess ||
+        cudaFuncSetAttribute(lag_pipe_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
         cudaFuncSetAttribute(lag_pipe_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
         cudaFuncSetAttribute(lag_pipe_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
+        cudaFuncSetAttribute(lag_pipe_kernel<20>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
+        cudaFuncSetAttribute(lag_pipe_kernel<24>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
+        cudaFuncSetAttribute(lag_pipe_kernel<30>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
         cudaFuncSetAttribute(lag_pipe_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess)
         return bail(fail(DDM_ERR_CUDA, "cudaFuncSetAttribute failed"));
 

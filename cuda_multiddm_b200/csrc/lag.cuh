@@ -31,10 +31,14 @@ namespace ddm {
 constexpr int kLagBlock = 256;    // elements per CTA (= threads)
 constexpr int kLagSlots = 48;     // shared-memory frame slots (> kMaxJ)
 constexpr int kLagSmemMax = 220 * 1024;
+// Register-frame counts the kernel is instantiated for (a launch uses the smallest >= nreg).
+constexpr int kLagJs[] = {4, 8, 16, 20, 24, 30, 32};
+constexpr int kNumLagJs = sizeof(kLagJs) / sizeof(kLagJs[0]);
 
 // Lag table layout (ints): header, register frames, tau entries, union slots.
 constexpr int kTabNreg = 0, kTabNtau = 1, kTabNunion = 2, kTabReg = 3;
-constexpr int kTabEntries = kTabReg + 32;  // then ntau acc indices, ntau union starts, nunion ring slots
+constexpr int kTabEntries = kTabReg + 32;  // then ntau acc indices, ntau union starts,
+                                           // ntau full-window flags, nunion ring slots
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -88,18 +92,35 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     return true;
 }
 
+// Packed FP32x2 helpers (sm_100a): one instruction for both halves of a complex value.
+__device__ __forceinline__ unsigned long long f2_sub(unsigned long long a, unsigned long long b) {
+    unsigned long long d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+__device__ __forceinline__ unsigned long long f2_fma_sq(unsigned long long d, unsigned long long acc) {
+    unsigned long long r;
+    asm("fma.rn.f32x2 %0, %1, %1, %2;" : "=l"(r) : "l"(d), "l"(acc));
+    return r;
+}
+
+__device__ __forceinline__ float f2_hsum(unsigned long long v) {
+    return __uint_as_float(static_cast<unsigned>(v)) + __uint_as_float(static_cast<unsigned>(v >> 32));
+}
+
 template <int J>
 __global__ void __launch_bounds__(kLagBlock, 2)
     lag_pipe_kernel(const float2 *__restrict__ ring, float2 *__restrict__ acc, long long E,
                     const int *__restrict__ table, int *__restrict__ status) {
     extern __shared__ __align__(128) unsigned char smem[];
-    float2 *slots = reinterpret_cast<float2 *>(smem);
+    unsigned long long *slots = reinterpret_cast<unsigned long long *>(smem);
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + sizeof(float2) * kLagSlots * kLagBlock);
     int *abort_flag = reinterpret_cast<int *>(full + kLagSlots);
     int *tab = abort_flag + 1;
 
     const int tid = threadIdx.x;
-    const int ntab = kTabEntries + 2 * table[kTabNtau] + table[kTabNunion];
+    const int ntab = kTabEntries + 3 * table[kTabNtau] + table[kTabNunion];
     for (int i = tid; i < ntab; i += kLagBlock) tab[i] = table[i];
     if (tid == 0) {
         for (int i = 0; i < kLagSlots; i++) mbar_init(&full[i], 1);
@@ -111,7 +132,8 @@ __global__ void __launch_bounds__(kLagBlock, 2)
     const int nreg = tab[kTabNreg], ntau = tab[kTabNtau], nu = tab[kTabNunion];
     const int *ent_acc = tab + kTabEntries;
     const int *ent_ub = ent_acc + ntau;
-    const int *uslot = ent_ub + ntau;
+    const int *ent_full = ent_ub + ntau;
+    const int *uslot = ent_full + ntau;
     const long long e0 = static_cast<long long>(blockIdx.x) * kLagBlock;
     const long long k = e0 + tid;
     const bool valid = k < E;
@@ -137,35 +159,55 @@ __global__ void __launch_bounds__(kLagBlock, 2)
     };
     if (tid == 0) issue_upto(kLagSlots);
 
-    float2 r[J];
+    const unsigned long long *ring64 = reinterpret_cast<const unsigned long long *>(ring);
+    unsigned long long r[J];
 #pragma unroll
     for (int j = 0; j < J; j++) {
         const int s = j < nreg ? tab[kTabReg + j] : -1;
-        r[j] = (valid && s >= 0) ? __ldg(ring + static_cast<long long>(s) * E + k) : make_float2(0.f, 0.f);
+        r[j] = (valid && s >= 0) ? __ldg(ring64 + static_cast<long long>(s) * E + k) : 0ull;
     }
     const float2 zero = make_float2(0.f, 0.f);
     float2 a_cur = (valid && ntau > 0) ? acc[static_cast<long long>(ent_acc[0]) * E + k] : zero;
     float2 a_nxt = (valid && ntau > 1) ? acc[static_cast<long long>(ent_acc[1]) * E + k] : zero;
 
+    int waited = 0;  // union indices below this have been waited for by this thread
     bool ok = true;
     for (int e = 0; e < ntau; e++) {
         const float2 a_far = (valid && e + 2 < ntau) ? acc[static_cast<long long>(ent_acc[e + 2]) * E + k] : zero;
         const int ub = ent_ub[e];
+        // Wait once for each partner frame that enters the window with this entry.
+        const int wend = ub + nreg;
+        for (int u = waited > ub ? waited : ub; u < wend; u++) {
+            if (uslot[u] >= 0 && !mbar_wait_bounded(&full[u % kLagSlots], (u / kLagSlots) & 1)) {
+                ok = false;
+                break;
+            }
+        }
+        waited = wend;
         float sum = 0.f;
+        if (ok) {
+            const int s0 = ub % kLagSlots;
+            const int wrap = kLagSlots - s0;  // j >= wrap wraps to the start of the ring
+            const unsigned long long *lo = slots + s0 * kLagBlock + tid;
+            const unsigned long long *hi = lo - kLagSlots * kLagBlock;
+            if (ent_full[e]) {  // nreg == J, every register frame and partner present
+                unsigned long long acc2 = 0ull;
 #pragma unroll
-        for (int j = 0; j < J; j++) {
-            if (j < nreg && tab[kTabReg + j] >= 0) {
-                const int u = ub + j;
-                if (uslot[u] >= 0) {
-                    if (!mbar_wait_bounded(&full[u % kLagSlots], (u / kLagSlots) & 1)) {
-                        ok = false;
-                        break;
-                    }
-                    const float2 b = slots[(u % kLagSlots) * kLagBlock + tid];
-                    const float dx = r[j].x - b.x, dy = r[j].y - b.y;
-                    sum = fmaf(dx, dx, sum);
-                    sum = fmaf(dy, dy, sum);
+                for (int j = 0; j < J; j++) {
+                    const unsigned long long b = (j < wrap ? lo : hi)[j * kLagBlock];
+                    acc2 = f2_fma_sq(f2_sub(r[j], b), acc2);
                 }
+                sum = f2_hsum(acc2);
+            } else {
+                unsigned long long acc2 = 0ull;
+#pragma unroll
+                for (int j = 0; j < J; j++) {
+                    if (j < nreg && tab[kTabReg + j] >= 0 && uslot[ub + j] >= 0) {
+                        const unsigned long long b = (j < wrap ? lo : hi)[j * kLagBlock];
+                        acc2 = f2_fma_sq(f2_sub(r[j], b), acc2);
+                    }
+                }
+                sum = f2_hsum(acc2);
             }
         }
         if (!ok) atomicExch(abort_flag, 1);
