@@ -291,7 +291,7 @@ int launch_lag(ddm_engine *e, const Launch &L) {
     TimedRange tr(e, 1);
     switch (J) {
 #define LAG_CASE(JJ) \
-    case JJ: lag_pipe_kernel<JJ><<<blocks, kLagBlock, smem, e->stream>>>(e->ring, e->acc, e->E, td, e->status_d); break;
+    case JJ: lag_pipe_kernel<JJ><<<blocks, kLagThreads, smem, e->stream>>>(e->ring, e->acc, e->E, td, e->status_d); break;
         LAG_CASE(4) LAG_CASE(8) LAG_CASE(16) LAG_CASE(20) LAG_CASE(24) LAG_CASE(30) LAG_CASE(32)
 #undef LAG_CASE
         default: return fail(DDM_ERR_STATE, "internal: no lag kernel for this frame count");

@@ -18,7 +18,6 @@ namespace ddm {
 
 constexpr int kMaxScales = 16;
 constexpr int kFftThreads = 256;
-constexpr int kLagThreads = 256;
 constexpr int kAzThreads = 256;
 constexpr int kMaxJ = 32;  // frames held in registers by one lag-kernel thread
 

@@ -11,12 +11,14 @@
 // needs about 480 distinct partner frames instead of 30 * 64 = 1920 frame reads.
 //
 // Data movement (sm_100a). Partner frames stream through a ring of kLagSlots shared-memory
-// slots, one slot = the CTA's element block of one frame (2 KB), each filled by a single
+// slots, one slot = the CTA's element block of one frame (1 KB), each filled by a single
 // 1-D bulk copy (cp.async.bulk, the TMA's linear mode; no multicast) that completes on the
-// slot's mbarrier. Thread 0 is the producer; after every tau entry the CTA synchronises,
-// which frees every union index below the next entry's window, and thread 0 refills those
-// slots kLagSlots ahead. Accumulators (FP32 sum + Kahan compensation, 8 B) are loaded two
-// entries ahead with plain coalesced loads and written back once per entry.
+// slot's "full" mbarrier. A dedicated producer warp refills a slot once every consumer warp
+// has arrived on its "empty" mbarrier, i.e. has moved past the last window that reads it.
+// The ring is a power of two of slots, so a window position becomes a shared-memory address
+// with one add and one mask. The |dF|^2 arithmetic uses packed FP32x2 instructions.
+// Accumulators (FP32 sum + Kahan compensation, 8 B) are loaded three entries ahead with
+// plain coalesced loads and written back once per entry.
 //
 // Every mbarrier wait is bounded (about one second of clock cycles); a wait that runs out
 // sets *status to 1, and the CTA waits (bounded again) for its own copies in flight before
@@ -28,8 +30,14 @@
 
 namespace ddm {
 
-constexpr int kLagBlock = 256;    // elements per CTA (= threads)
-constexpr int kLagSlots = 48;     // shared-memory frame slots (> kMaxJ)
+constexpr int kLagBlock = 128;                     // elements per CTA, one per consumer thread
+constexpr int kLagConsumerWarps = kLagBlock / 32;
+constexpr int kLagThreads = kLagBlock + 32;        // consumers + one producer warp
+constexpr int kLagSlotsLog2 = 6;
+constexpr int kLagSlots = 1 << kLagSlotsLog2;      // shared-memory frame slots (> 32 frames)
+constexpr uint32_t kLagSlotBytes = kLagBlock * 8;  // one frame of the CTA's elements
+constexpr uint32_t kLagRingBytes = kLagSlots * kLagSlotBytes;
+constexpr uint32_t kLagRingMask = kLagRingBytes - kLagSlotBytes;  // slot bits of a ring offset
 constexpr int kLagSmemMax = 220 * 1024;
 // Register-frame counts the kernel is instantiated for (a launch uses the smallest >= nreg).
 constexpr int kLagJs[] = {4, 8, 16, 20, 24, 30, 32};
@@ -109,21 +117,29 @@ __device__ __forceinline__ float f2_hsum(unsigned long long v) {
     return __uint_as_float(static_cast<unsigned>(v)) + __uint_as_float(static_cast<unsigned>(v >> 32));
 }
 
+// Warp-specialised pipeline. Warps 0..kLagConsumerWarps-1 consume (one spectrum element
+// per thread); the last warp produces (its lane 0 issues the bulk copies). Per ring slot,
+// full[slot] completes when the slot's frame has landed and empty[slot] when every consumer
+// warp has released it, so neither side ever waits for the whole CTA.
 template <int J>
-__global__ void __launch_bounds__(kLagBlock, 2)
+__global__ void __launch_bounds__(kLagThreads, 3)
     lag_pipe_kernel(const float2 *__restrict__ ring, float2 *__restrict__ acc, long long E,
                     const int *__restrict__ table, int *__restrict__ status) {
-    extern __shared__ __align__(128) unsigned char smem[];
-    unsigned long long *slots = reinterpret_cast<unsigned long long *>(smem);
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem + sizeof(float2) * kLagSlots * kLagBlock);
-    int *abort_flag = reinterpret_cast<int *>(full + kLagSlots);
-    int *tab = abort_flag + 1;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + kLagRingBytes);
+    uint64_t *empty = full + kLagSlots;
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(empty + kLagSlots);
+    int *tab = const_cast<int *>(reinterpret_cast<volatile int *>(abort_flag + 1));
 
     const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
     const int ntab = kTabEntries + 3 * table[kTabNtau] + table[kTabNunion];
-    for (int i = tid; i < ntab; i += kLagBlock) tab[i] = table[i];
+    for (int i = tid; i < ntab; i += kLagThreads) tab[i] = table[i];
     if (tid == 0) {
-        for (int i = 0; i < kLagSlots; i++) mbar_init(&full[i], 1);
+        for (int i = 0; i < kLagSlots; i++) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], kLagConsumerWarps);
+        }
         *abort_flag = 0;
         fence_mbar_init();
     }
@@ -135,110 +151,114 @@ __global__ void __launch_bounds__(kLagBlock, 2)
     const int *ent_full = ent_ub + ntau;
     const int *uslot = ent_full + ntau;
     const long long e0 = static_cast<long long>(blockIdx.x) * kLagBlock;
-    const long long k = e0 + tid;
-    const bool valid = k < E;
-    const uint32_t bytes = static_cast<uint32_t>(
-        sizeof(float2) * (E - e0 < kLagBlock ? E - e0 : static_cast<long long>(kLagBlock)));
 
-    // Producer state lives in thread 0 only. Union index u is the (u / kLagSlots)-th use of
-    // slot u % kLagSlots, and every use completes exactly one phase of the slot's barrier:
-    // a copy's transaction bytes, or a bare arrival when there is no frame to copy.
-    int issued = 0;
-    auto issue_upto = [&](int limit) {
-        for (; issued < nu && issued < limit; issued++) {
-            const int s = uslot[issued];
-            uint64_t *bar = &full[issued % kLagSlots];
-            if (s < 0) {  // no such frame: nothing to copy, nobody waits; keep the phase count
-                mbar_arrive(bar);
-                continue;
+    if (warp == kLagConsumerWarps) {
+        // ---------------- producer: union index u is fill u / kLagSlots of slot u % kLagSlots
+        if (lane == 0) {
+            const uint32_t bytes = static_cast<uint32_t>(
+                sizeof(float2) * (E - e0 < kLagBlock ? E - e0 : static_cast<long long>(kLagBlock)));
+            for (int u = 0; u < nu; u++) {
+                const int slot = u & (kLagSlots - 1), fill = u >> kLagSlotsLog2;
+                if (fill > 0 && !mbar_wait_bounded(&empty[slot], (fill - 1) & 1)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                if (*abort_flag) break;
+                const int s = uslot[u];
+                if (s < 0) {  // no such frame: complete the phase without data, nobody reads it
+                    mbar_arrive(&full[slot]);
+                    continue;
+                }
+                mbar_expect_tx(&full[slot], bytes);
+                bulk_load(smem + slot * kLagSlotBytes, ring + static_cast<long long>(s) * E + e0, bytes, &full[slot]);
             }
-            mbar_expect_tx(bar, bytes);
-            bulk_load(slots + (issued % kLagSlots) * kLagBlock, ring + static_cast<long long>(s) * E + e0, bytes,
-                      bar);
         }
-    };
-    if (tid == 0) issue_upto(kLagSlots);
-
-    const unsigned long long *ring64 = reinterpret_cast<const unsigned long long *>(ring);
-    unsigned long long r[J];
+    } else {
+        // ---------------- consumers
+        const long long k = e0 + tid;
+        const bool valid = k < E;
+        const uint32_t toff = static_cast<uint32_t>(tid) * sizeof(float2);
+        const unsigned long long *ring64 = reinterpret_cast<const unsigned long long *>(ring);
+        unsigned long long r[J];
 #pragma unroll
-    for (int j = 0; j < J; j++) {
-        const int s = j < nreg ? tab[kTabReg + j] : -1;
-        r[j] = (valid && s >= 0) ? __ldg(ring64 + static_cast<long long>(s) * E + k) : 0ull;
-    }
-    const float2 zero = make_float2(0.f, 0.f);
-    float2 a_cur = (valid && ntau > 0) ? acc[static_cast<long long>(ent_acc[0]) * E + k] : zero;
-    float2 a_nxt = (valid && ntau > 1) ? acc[static_cast<long long>(ent_acc[1]) * E + k] : zero;
-
-    int waited = 0;  // union indices below this have been waited for by this thread
-    bool ok = true;
-    for (int e = 0; e < ntau; e++) {
-        const float2 a_far = (valid && e + 2 < ntau) ? acc[static_cast<long long>(ent_acc[e + 2]) * E + k] : zero;
-        const int ub = ent_ub[e];
-        // Wait once for each partner frame that enters the window with this entry.
-        const int wend = ub + nreg;
-        for (int u = waited > ub ? waited : ub; u < wend; u++) {
-            if (uslot[u] >= 0 && !mbar_wait_bounded(&full[u % kLagSlots], (u / kLagSlots) & 1)) {
-                ok = false;
-                break;
-            }
+        for (int j = 0; j < J; j++) {
+            const int s = j < nreg ? tab[kTabReg + j] : -1;
+            r[j] = (valid && s >= 0) ? __ldg(ring64 + static_cast<long long>(s) * E + k) : 0ull;
         }
-        waited = wend;
-        float sum = 0.f;
-        if (ok) {
-            const int s0 = ub % kLagSlots;
-            const int wrap = kLagSlots - s0;  // j >= wrap wraps to the start of the ring
-            const unsigned long long *lo = slots + s0 * kLagBlock + tid;
-            const unsigned long long *hi = lo - kLagSlots * kLagBlock;
+        const float2 zero = make_float2(0.f, 0.f);
+        float2 a0 = (valid && ntau > 0) ? acc[static_cast<long long>(ent_acc[0]) * E + k] : zero;
+        float2 a1 = (valid && ntau > 1) ? acc[static_cast<long long>(ent_acc[1]) * E + k] : zero;
+        float2 a2 = (valid && ntau > 2) ? acc[static_cast<long long>(ent_acc[2]) * E + k] : zero;
+        int waited = 0, released = 0;
+        for (int e = 0; e < ntau; e++) {
+            const float2 a3 = (valid && e + 3 < ntau) ? acc[static_cast<long long>(ent_acc[e + 3]) * E + k] : zero;
+            const int ub = ent_ub[e];
+            bool ok = true;
+            for (int u = waited > ub ? waited : ub; u < ub + nreg; u++) {  // frames new to this window
+                if (uslot[u] >= 0 && !mbar_wait_bounded(&full[u & (kLagSlots - 1)], (u >> kLagSlotsLog2) & 1)) {
+                    ok = false;
+                    break;
+                }
+            }
+            waited = ub + nreg;
+            if (!ok) *abort_flag = 1;
+            if (*abort_flag) break;
+            const uint32_t o = static_cast<uint32_t>(ub) * kLagSlotBytes;
+            unsigned long long acc2 = 0ull;
             if (ent_full[e]) {  // nreg == J, every register frame and partner present
-                unsigned long long acc2 = 0ull;
 #pragma unroll
                 for (int j = 0; j < J; j++) {
-                    const unsigned long long b = (j < wrap ? lo : hi)[j * kLagBlock];
+                    const uint32_t off = ((o + j * kLagSlotBytes) & kLagRingMask) | toff;
+                    const unsigned long long b = *reinterpret_cast<const unsigned long long *>(smem + off);
                     acc2 = f2_fma_sq(f2_sub(r[j], b), acc2);
                 }
-                sum = f2_hsum(acc2);
             } else {
-                unsigned long long acc2 = 0ull;
 #pragma unroll
                 for (int j = 0; j < J; j++) {
                     if (j < nreg && tab[kTabReg + j] >= 0 && uslot[ub + j] >= 0) {
-                        const unsigned long long b = (j < wrap ? lo : hi)[j * kLagBlock];
+                        const uint32_t off = ((o + j * kLagSlotBytes) & kLagRingMask) | toff;
+                        const unsigned long long b = *reinterpret_cast<const unsigned long long *>(smem + off);
                         acc2 = f2_fma_sq(f2_sub(r[j], b), acc2);
                     }
                 }
-                sum = f2_hsum(acc2);
             }
-        }
-        if (!ok) atomicExch(abort_flag, 1);
-        // Kahan step: a.x running sum, a.y compensation (true value a.x - a.y)
-        const float y = sum - a_cur.y;
-        const float t = a_cur.x + y;
-        a_cur.y = (t - a_cur.x) - y;
-        a_cur.x = t;
-        if (valid && ok) acc[static_cast<long long>(ent_acc[e]) * E + k] = a_cur;
-        a_cur = a_nxt;
-        a_nxt = a_far;
-        __syncthreads();  // every thread is done with union indices below the next window
-        if (*abort_flag) break;
-        if (tid == 0) {
-            fence_proxy_async_smem();
-            issue_upto((e + 1 < ntau ? ent_ub[e + 1] : nu) + kLagSlots);
+            const float sum = f2_hsum(acc2);
+            // Kahan step: a.x running sum, a.y compensation (true value a.x - a.y)
+            const float y = sum - a0.y;
+            const float t = a0.x + y;
+            a0.y = (t - a0.x) - y;
+            a0.x = t;
+            if (valid) acc[static_cast<long long>(ent_acc[e]) * E + k] = a0;
+            a0 = a1;
+            a1 = a2;
+            a2 = a3;
+            // release the slots no later entry reads
+            const int next = e + 1 < ntau ? ent_ub[e + 1] : nu;
+            __syncwarp();
+            if (lane == 0)
+                for (; released < next; released++) mbar_arrive(&empty[released & (kLagSlots - 1)]);
         }
     }
+    __syncthreads();
     if (*abort_flag) {
         if (tid == 0) {
             atomicExch(status, 1);
-            // drain: wait (bounded) for the copies this CTA issued into its own shared memory
-            for (int u = issued - 1; u >= 0 && u >= issued - kLagSlots; u--)
-                if (uslot[u] >= 0) mbar_wait_bounded(&full[u % kLagSlots], (u / kLagSlots) & 1);
+            // drain: wait (bounded) until every copy this CTA issued has landed
+            for (int slot = 0; slot < kLagSlots; slot++) {
+                for (int u = slot; u < nu; u += kLagSlots) {
+                    if (uslot[u] >= 0 && !mbar_try_wait(&full[slot], (u >> kLagSlotsLog2) & 1)) {
+                        mbar_wait_bounded(&full[slot], (u >> kLagSlotsLog2) & 1);
+                        break;
+                    }
+                }
+            }
         }
         __syncthreads();
     }
 }
 
 inline size_t lag_smem_bytes(int table_ints) {
-    return sizeof(float2) * kLagSlots * kLagBlock + sizeof(uint64_t) * kLagSlots + sizeof(int) * (1 + table_ints);
+    return kLagRingBytes + 2 * sizeof(uint64_t) * kLagSlots + sizeof(int) * (1 + table_ints);
 }
 
 }  // namespace ddm
