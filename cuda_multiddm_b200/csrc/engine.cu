@@ -22,6 +22,7 @@
 #include "../../include/ddm.h"
 #include "errors.hpp"
 #include "host.hpp"
+#include "fft.cuh"
 #include "kernels.cuh"
 #include "lag.cuh"
 
@@ -178,57 +179,60 @@ struct TimedRange {
 
 int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long long row_pitch,
                int x_off, int y_off, int nframes, long long first_label) {
-    const int log2tw = log2i(e->scales[0]);
     TimedRange tr(e, 0);
-    for (const ScaleDesc &d : e->sd) {
-        const int s = d.s, log2s = log2i(s);
-        RowArgs ra;
-        ra.src = src;
-        ra.frame_stride = frame_stride;
-        ra.row_pitch = row_pitch;
-        ra.bpp = e->bpp;
-        ra.pixmode = e->pixmode;
-        ra.x_off = x_off;
-        ra.y_off = y_off;
-        ra.s = s;
-        ra.log2s = log2s;
-        ra.tiles_side = e->M / s;
-        ra.pairs_per_cta = std::max(1, std::min(s / 2, 2048 / s));
-        ra.ctas_per_tile = (s / 2) / ra.pairs_per_cta;
-        ra.n = d.n;
-        ra.off = d.off;
-        ra.E = e->E;
-        ra.first_label = first_label;
-        ra.R = e->R;
-        ra.ring = e->ring;
-        ra.tw = e->tw;
-        ra.log2tw = log2tw;
-        dim3 grid(d.tiles * ra.ctas_per_tile, nframes);
-        size_t smem = sizeof(float2) * ra.pairs_per_cta * s;
-        fft_rows_kernel<<<grid, kFftThreads, smem, e->stream>>>(ra);
-        CUDA_TRY(cudaGetLastError());
-        e->launches++;
-
-        ColArgs ca;
-        ca.s = s;
-        ca.log2s = log2s;
-        ca.P = std::min(16, std::max(1, 16384 / s));
-        ca.groups_per_tile = (s / 2 + 1 + ca.P - 1) / ca.P;
-        ca.n = d.n;
-        ca.off = d.off;
-        ca.E = e->E;
-        ca.first_label = first_label;
-        ca.R = e->R;
-        ca.ring = e->ring;
-        ca.tw = e->tw;
-        ca.log2tw = log2tw;
-        dim3 cgrid(d.tiles * ca.groups_per_tile, nframes);
-        size_t csmem = sizeof(float2) * ca.P * s;
-        fft_cols_kernel<<<cgrid, kFftThreads, csmem, e->stream>>>(ca);
-        CUDA_TRY(cudaGetLastError());
-        e->launches++;
+    FftArgs rows, cols;
+    std::memset(&rows, 0, sizeof(rows));
+    rows.S = e->S;
+    rows.src = src;
+    rows.frame_stride = frame_stride;
+    rows.row_pitch = row_pitch;
+    rows.bpp = e->bpp;
+    rows.pixmode = e->pixmode;
+    rows.x_off = x_off;
+    rows.y_off = y_off;
+    rows.ring = e->ring;
+    rows.E = e->E;
+    rows.R = e->R;
+    rows.tw = e->tw;
+    rows.log2M = log2i(e->M);
+    cols = rows;
+    int row_ctas = 0, col_ctas = 0;
+    size_t smem = 0;
+    for (int si = 0; si < e->S; si++) {
+        const ScaleDesc &d = e->sd[si];
+        const int s = d.s, per = fft_per_cta(s), side = e->M / s;
+        FftScale fs;
+        fs.s = s;
+        fs.log2s = log2i(s);
+        fs.tiles_side = side;
+        fs.n = d.n;
+        fs.off = d.off;
+        fs.cta_begin = row_ctas;
+        fs.ctas_per_frame = static_cast<int>((static_cast<long long>(d.tiles) * (s / 2) + per - 1) / per);
+        rows.sc[si] = fs;
+        row_ctas += fs.ctas_per_frame;
+        fs.cta_begin = col_ctas;
+        fs.ctas_per_frame = static_cast<int>((static_cast<long long>(d.tiles) * (s / 2 + 1) + per - 1) / per);
+        cols.sc[si] = fs;
+        col_ctas += fs.ctas_per_frame;
+        smem = std::max(smem, fft_smem_bytes(s));
     }
-    tr.end(2L * e->S);
+    // Frames go through both passes in groups small enough for the row pass's output to
+    // stay in L2 until the column pass reads it.
+    const long long frame_bytes = e->E * static_cast<long long>(sizeof(float2));
+    const int group = static_cast<int>(std::max<long long>(1, std::min<long long>(nframes, (64LL << 20) / frame_bytes)));
+    for (int f0 = 0; f0 < nframes; f0 += group) {
+        const int nf = std::min(group, nframes - f0);
+        rows.src = src + f0 * frame_stride;
+        rows.first_label = cols.first_label = first_label + f0;
+        fft_rows_kernel<<<dim3(row_ctas, nf), kFftThreads, smem, e->stream>>>(rows);
+        CUDA_TRY(cudaGetLastError());
+        fft_cols_kernel<<<dim3(col_ctas, nf), kFftThreads, smem, e->stream>>>(cols);
+        CUDA_TRY(cudaGetLastError());
+        e->launches += 2;
+        tr.e->tlaunch[0] += 2;
+    }
+    tr.end(0);
     return DDM_OK;
 }
 
@@ -488,7 +492,8 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
                                                 /*enforce_lambda_scale=*/compat, nullptr);
     if (!msg.empty()) return bail(fail(DDM_ERR_INVALID_ARG, msg));
     e->M = e->scales[0];
-    if (e->M > 16384) return bail(fail(DDM_ERR_INVALID_ARG, "the largest scale must be <= 16384"));
+    if (e->M > (1 << kFftMaxLog2))
+        return bail(fail(DDM_ERR_INVALID_ARG, "the largest scale must be <= " + std::to_string(1 << kFftMaxLog2)));
     if (e->M + e->x_off > e->w || e->M + e->y_off > e->h || e->x_off < 0 || e->y_off < 0)
         return bail(fail(DDM_ERR_INVALID_ARG, "the specified out dimensions must be smaller than actual image size"));
     if (e->scales.back() < 2) return bail(fail(DDM_ERR_INVALID_ARG, "scales must be at least 2"));
@@ -584,11 +589,11 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
         if (cudaEventCreateWithFlags(&e->tab_ev[i], cudaEventDisableTiming) != cudaSuccess)
             return bail(fail(DDM_ERR_CUDA, "cudaEventCreate failed"));
 
-    // Twiddles e^{-2 pi i m / M}, m < M/2, from FP64 math rounded to FP32
+    // Twiddles e^{-2 pi i m / M}, m < M, from FP64 math rounded to FP32
     {
-        std::vector<float2> tw(std::max(1, e->M / 2));
+        std::vector<float2> tw(e->M);
         const double two_pi = 6.283185307179586476925286766559;
-        for (int m = 0; m < e->M / 2; m++) {
+        for (int m = 0; m < e->M; m++) {
             double a = two_pi * m / e->M;
             tw[m] = make_float2(static_cast<float>(std::cos(a)), static_cast<float>(-std::sin(a)));
         }
@@ -620,8 +625,8 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
     }
 
     // Kernel shared-memory limits (the FFT passes use up to 128 KB)
-    if (cudaFuncSetAttribute(fft_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024) != cudaSuccess ||
-        cudaFuncSetAttribute(fft_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024) != cudaSuccess ||
+    if (cudaFuncSetAttribute(fft_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024) != cudaSuccess ||
+        cudaFuncSetAttribute(fft_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024) != cudaSuccess ||
         cudaFuncSetAttribute(lag_pipe_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
         cudaFuncSetAttribute(lag_pipe_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
         cudaFuncSetAttribute(lag_pipe_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||

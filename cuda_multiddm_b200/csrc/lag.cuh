@@ -20,7 +20,7 @@
 // Accumulators (FP32 sum + Kahan compensation, 8 B) are loaded three entries ahead with
 // plain coalesced loads and written back once per entry.
 //
-// Every mbarrier wait is bounded (about one second of clock cycles); a wait that runs out
+// Every mbarrier wait is bounded (kWaitCycles clock cycles); a wait that runs out
 // sets *status to 1, and the CTA waits (bounded again) for its own copies in flight before
 // returning, so a broken schedule ends the kernel instead of hanging the GPU.
 #pragma once
@@ -91,12 +91,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait: false if the phase did not complete within ~1 s of SM clocks.
+// Bounded wait: false if the phase did not complete within kWaitCycles SM clocks (about
+// 0.2 s at 2 GHz, four orders of magnitude above any legitimate copy latency).
+constexpr long long kWaitCycles = 400000000LL;
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity))
-        if (clock64() - t0 > 2000000000LL) return false;
+        if (clock64() - t0 > kWaitCycles) return false;
     return true;
 }
 
@@ -194,8 +196,12 @@ __global__ void __launch_bounds__(kLagThreads, 3)
             const float2 a3 = (valid && e + 3 < ntau) ? acc[static_cast<long long>(ent_acc[e + 3]) * E + k] : zero;
             const int ub = ent_ub[e];
             bool ok = true;
-            for (int u = waited > ub ? waited : ub; u < ub + nreg; u++) {  // frames new to this window
-                if (uslot[u] >= 0 && !mbar_wait_bounded(&full[u & (kLagSlots - 1)], (u >> kLagSlotsLog2) & 1)) {
+            // Wait for the entries new to this window, those without a frame included (the
+            // producer's bare arrival): a consumer must never release a fill of a slot that
+            // the producer has not issued yet, or the slot's empty barrier would run a phase
+            // ahead of the producer's parity.
+            for (int u = waited > ub ? waited : ub; u < ub + nreg; u++) {
+                if (!mbar_wait_bounded(&full[u & (kLagSlots - 1)], (u >> kLagSlotsLog2) & 1)) {
                     ok = false;
                     break;
                 }

@@ -72,7 +72,7 @@ def frames_digest(frames: np.ndarray) -> str:
 
 
 CASES = [
-    # BASELINE config 1 shape: 200 frames 256^2, one 256 tile, tau 1..20, 10 lambdas 4..128
+    # the plain single-scale workload: 200 frames 256^2, one 256 tile, tau 1..20, 10 lambdas 4..128
     Case("c1_plain", 1001, 256, 256, 200, [256], list(range(1, 21)),
          [4.0, 5.87, 8.62, 12.7, 18.6, 27.3, 40.1, 58.8, 86.3, 126.7], N=200, C=20, spots=300),
     # four scales, every tile (T = 1), ROI offset inside a larger frame, 25% tolerance
