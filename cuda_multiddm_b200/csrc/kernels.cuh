@@ -18,14 +18,6 @@ constexpr int kMaxScales = 16;
 constexpr int kAzThreads = 256;
 constexpr int kMaxJ = 32;  // frames held in registers by one lag-kernel thread
 
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-
-__device__ __forceinline__ unsigned bitrev(unsigned k, int log2n) {
-    return log2n == 0 ? 0u : (__brev(k) >> (32 - log2n));
-}
-
 struct ScaleDesc {
     int s, tiles;
     long long n, off;     // elements per tile, offset of the scale in a frame
