@@ -177,6 +177,7 @@ def test_errors_are_status_codes():
 def test_kernel_launches_counted():
     frames = media.synth_video(2, 64, 64, 8, 10)
     _, _, info = engine_run(frames, [64, 32], [1, 2], [4.0], estimator="unbiased", C=4)
-    # per piece of 4 frames: 2 FFT passes per scale + 1 lag launch; 1 azimuthal launch
-    assert info.kernel_launches == 2 * (2 * 2 + 1) + 1
+    # per piece of 4 frames: one row-pass and one column-pass launch over all scales (the
+    # 4 frames fit one L2-resident group) + 1 lag launch; then 1 azimuthal launch
+    assert info.kernel_launches == 2 * (2 + 1) + 1
     assert lib() is not None
