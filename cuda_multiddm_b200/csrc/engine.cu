@@ -25,6 +25,7 @@
 #include "fft.cuh"
 #include "kernels.cuh"
 #include "lag.cuh"
+#include "lag_host.hpp"
 
 namespace ddm {
 
@@ -47,7 +48,7 @@ namespace {
 
 constexpr int kTables = 64;  // lag tables in flight
 
-struct Launch {  // one lag-kernel launch: register frames, tau windows, position slots
+struct Launch {  // one lag-kernel launch: register frames, tau windows (ascending), position slots
     int nreg = 0;
     int reg[kMaxJ];
     std::vector<int> ent_acc, ent_w, pos;
@@ -86,6 +87,7 @@ struct ddm_engine {
     int *q_ptr_d = nullptr, *idx_d = nullptr, *counts_d = nullptr;
     double *norm_d = nullptr, *isf_d = nullptr;
     int *status_d = nullptr;                // set by kernels whose bounded waits ran out
+    LagMaps maps;                           // 2-D tensor maps of the ring for the lag kernel
     size_t device_bytes = 0;
     std::vector<int> counts_h;             // [S][Q]
     std::vector<std::vector<int>> q_ptr_s, idx_s;  // per scale CSR (host copy)
@@ -240,51 +242,20 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
 // Lag launches
 // ---------------------------------------------------------------------------------
 
-// Entries must come with ascending window starts (ent_w). The windows of all entries
-// are merged into the sorted list of distinct partner positions (the union); entry e's
-// window is then union indices [ub_e, ub_e + nreg), always the tail of the list at the
-// time the entry is appended, because windows are contiguous and start in order.
 int launch_lag(ddm_engine *e, const Launch &L) {
     if (L.nreg <= 0 || L.ent_acc.empty()) return DDM_OK;
-    const int ntau = static_cast<int>(L.ent_acc.size());
-    std::vector<int> ub(ntau), uslot;
-    uslot.reserve(L.pos.size());
-    int next = std::numeric_limits<int>::min();  // first position past the union so far
-    for (int i = 0; i < ntau; i++) {
-        const int w = L.ent_w[i];
-        if (i > 0 && w <= L.ent_w[i - 1]) return fail(DDM_ERR_STATE, "internal: lag windows out of order");
-        for (int p = std::max(w, next); p < w + L.nreg; p++) uslot.push_back(L.pos[p]);
-        next = std::max(next, w + L.nreg);
-        ub[i] = static_cast<int>(uslot.size()) - L.nreg;
-    }
-    const int nu = static_cast<int>(uslot.size());
-    // Register-frame count the kernel is compiled for; entries whose whole window is present
-    // and that use all J register frames take the kernel's unchecked fast path.
-    int J = kLagJs[kNumLagJs - 1];
-    for (int i = kNumLagJs - 1; i >= 0; i--)
-        if (kLagJs[i] >= L.nreg) J = kLagJs[i];
-    bool regs_ok = L.nreg == J;
-    for (int j = 0; j < L.nreg; j++) regs_ok = regs_ok && L.reg[j] >= 0;
-    std::vector<int> full(ntau);
-    for (int i = 0; i < ntau; i++) {
-        bool f = regs_ok;
-        for (int j = 0; j < L.nreg && f; j++) f = uslot[ub[i] + j] >= 0;
-        full[i] = f ? 1 : 0;
-    }
-    const int ntab = kTabEntries + 3 * ntau + nu;
+    const int J = lag_pick_j(L.nreg);
+    if (J == 0) return fail(DDM_ERR_STATE, "internal: no lag kernel for this frame count");
+    std::vector<int> table;
+    std::string err = build_lag_table(L.nreg, L.reg, L.ent_acc, L.ent_w, L.pos, J, &table);
+    if (!err.empty()) return fail(DDM_ERR_STATE, "internal: " + err);
+    const int ntab = static_cast<int>(table.size());
     if (ntab > e->tab_stride) return fail(DDM_ERR_STATE, "internal: lag table overflow");
     const int ts = e->tab_next;
     e->tab_next = (e->tab_next + 1) % kTables;
     if (e->tab_used[ts]) CUDA_TRY(cudaEventSynchronize(e->tab_ev[ts]));
     int *th = e->tables_h + static_cast<size_t>(ts) * e->tab_stride;
-    th[kTabNreg] = L.nreg;
-    th[kTabNtau] = ntau;
-    th[kTabNunion] = nu;
-    for (int j = 0; j < kMaxJ; j++) th[kTabReg + j] = j < L.nreg ? L.reg[j] : -1;
-    std::copy(L.ent_acc.begin(), L.ent_acc.end(), th + kTabEntries);
-    std::copy(ub.begin(), ub.end(), th + kTabEntries + ntau);
-    std::copy(full.begin(), full.end(), th + kTabEntries + 2 * ntau);
-    std::copy(uslot.begin(), uslot.end(), th + kTabEntries + 3 * ntau);
+    std::copy(table.begin(), table.end(), th);
     int *td = e->tables_d + static_cast<size_t>(ts) * e->tab_stride;
     CUDA_TRY(cudaMemcpyAsync(td, th, sizeof(int) * ntab, cudaMemcpyHostToDevice, e->stream));
     CUDA_TRY(cudaEventRecord(e->tab_ev[ts], e->stream));
@@ -294,8 +265,11 @@ int launch_lag(ddm_engine *e, const Launch &L) {
     const size_t smem = lag_smem_bytes(ntab);
     TimedRange tr(e, 1);
     switch (J) {
-#define LAG_CASE(JJ) \
-    case JJ: lag_pipe_kernel<JJ><<<blocks, kLagThreads, smem, e->stream>>>(e->ring, e->acc, e->E, td, e->status_d); break;
+#define LAG_CASE(JJ)                                                                                   \
+    case JJ:                                                                                           \
+        lag_pipe_kernel<JJ><<<blocks, kLagThreads, smem, e->stream>>>(e->ring, e->acc, e->E, td, e->status_d, \
+                                                                       e->maps);                        \
+        break;
         LAG_CASE(4) LAG_CASE(8) LAG_CASE(16) LAG_CASE(20) LAG_CASE(24) LAG_CASE(30) LAG_CASE(32)
 #undef LAG_CASE
         default: return fail(DDM_ERR_STATE, "internal: no lag kernel for this frame count");
@@ -503,9 +477,8 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
     e->T = static_cast<int>(e->taus.size());
     e->Q = static_cast<int>(e->lambdas.size());
     e->tau_max = e->taus.back();
-    if (lag_smem_bytes(kTabEntries + 3 * e->T + kMaxJ + e->tau_max) > static_cast<size_t>(kLagSmemMax))
-        return bail(fail(DDM_ERR_INVALID_ARG, "tau list too long: 2 * tau_count + tau_max must stay below " +
-                                                  std::to_string((kLagSmemMax - lag_smem_bytes(kTabEntries + kMaxJ)) / 4)));
+    if (lag_smem_bytes(lag_table_capacity(e->T, kMaxJ + e->tau_max)) > static_cast<size_t>(kLagSmemMax))
+        return bail(fail(DDM_ERR_INVALID_ARG, "tau list too long for the lag kernel's shared-memory table"));
 
     // Geometry
     long long off = 0, isf_off = 0;
@@ -550,7 +523,7 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
     const size_t ring_bytes = sizeof(float2) * static_cast<size_t>(e->R) * e->E;
     const size_t acc_bytes = sizeof(float2) * static_cast<size_t>(e->T) * e->E;
     const size_t stage_bytes = static_cast<size_t>(e->jmax) * e->M * e->M * e->bpp;
-    e->tab_stride = kTabEntries + 3 * e->T + kMaxJ + e->tau_max + 4;
+    e->tab_stride = lag_table_capacity(e->T, kMaxJ + e->tau_max);
     size_t need = ring_bytes + acc_bytes + stage_bytes + sizeof(double) * e->isf_size +
                   sizeof(int) * static_cast<size_t>(kTables) * e->tab_stride;
     if (cfg->hbm_budget_bytes && need > cfg->hbm_budget_bytes)
@@ -575,6 +548,10 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
     }
     int st;
     if ((st = dev_alloc(e, &e->ring, static_cast<size_t>(e->R) * e->E))) return bail(st);
+    {
+        std::string err = make_lag_maps(e->ring, e->E, e->R, &e->maps);
+        if (!err.empty()) return bail(fail(DDM_ERR_CUDA, err));
+    }
     if ((st = dev_alloc(e, &e->acc, static_cast<size_t>(e->T) * e->E))) return bail(st);
     if ((st = dev_alloc(e, &e->stage, stage_bytes))) return bail(st);
     if ((st = dev_alloc(e, &e->tables_d, static_cast<size_t>(kTables) * e->tab_stride))) return bail(st);

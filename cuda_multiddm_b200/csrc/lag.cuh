@@ -11,10 +11,12 @@
 // needs about 480 distinct partner frames instead of 30 * 64 = 1920 frame reads.
 //
 // Data movement (sm_100a). Partner frames stream through a ring of kLagSlots shared-memory
-// slots, one slot = the CTA's element block of one frame (1 KB), each filled by a single
-// 1-D bulk copy (cp.async.bulk, the TMA's linear mode; no multicast) that completes on the
-// slot's "full" mbarrier. A dedicated producer warp refills a slot once every consumer warp
-// has arrived on its "empty" mbarrier, i.e. has moved past the last window that reads it.
+// slots, one slot = the CTA's element block of one frame (1 KB), grouped by kLagGroup. The
+// ring in HBM is addressed through 2-D tensor maps ([slots][elements], boxes of 1..8 slots
+// x kLagBlock elements), so a run of consecutive frames arrives with one
+// cp.async.bulk.tensor.2d (no multicast) that completes on the group's "full" mbarrier. A
+// dedicated producer warp refills a group once every consumer warp has arrived on its
+// "empty" mbarrier, i.e. has moved past the last window that reads it.
 // The ring is a power of two of slots, so a window position becomes a shared-memory address
 // with one add and one mask. The |dF|^2 arithmetic uses packed FP32x2 instructions.
 // Accumulators (FP32 sum + Kahan compensation, 8 B) are loaded three entries ahead with
@@ -26,6 +28,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace ddm {
@@ -43,10 +46,29 @@ constexpr int kLagSmemMax = 220 * 1024;
 constexpr int kLagJs[] = {4, 8, 16, 20, 24, 30, 32};
 constexpr int kNumLagJs = sizeof(kLagJs) / sizeof(kLagJs[0]);
 
-// Lag table layout (ints): header, register frames, tau entries, union slots.
-constexpr int kTabNreg = 0, kTabNtau = 1, kTabNunion = 2, kTabReg = 3;
-constexpr int kTabEntries = kTabReg + 32;  // then ntau acc indices, ntau union starts,
-                                           // ntau full-window flags, nunion ring slots
+// Union entries are copied in groups of kLagGroup consecutive entries; a group's ring
+// slots arrive as runs of 1, 2, 4 or 8 consecutive slots (one 2-D TMA box each).
+constexpr int kLagGroupLog2 = 3;
+constexpr int kLagGroup = 1 << kLagGroupLog2;
+constexpr int kLagGroupSlotsLog2 = kLagSlotsLog2 - kLagGroupLog2;
+constexpr int kLagGroupSlots = 1 << kLagGroupSlotsLog2;
+constexpr int kLagRunKinds = 4;  // box heights 1, 2, 4, 8
+
+// A run: ring slot in bits 0..19, log2(rows) in bits 20..21, position in its group in 22..24.
+__host__ __device__ constexpr int lag_run(int rel, int slot, int log2rows) {
+    return slot | (log2rows << 20) | (rel << 22);
+}
+__host__ __device__ constexpr int lag_run_slot(int run) { return run & 0xFFFFF; }
+__host__ __device__ constexpr int lag_run_log2rows(int run) { return (run >> 20) & 3; }
+__host__ __device__ constexpr int lag_run_rel(int run) { return (run >> 22) & 7; }
+
+// Lag table layout (ints): header, register frames, then ntau accumulator indices, ntau
+// union starts, ntau full-window flags, nunion ring slots, ngroups+1 run offsets, nruns runs.
+constexpr int kTabNreg = 0, kTabNtau = 1, kTabNunion = 2, kTabNgroups = 3, kTabNruns = 4, kTabReg = 5;
+constexpr int kTabEntries = kTabReg + 32;
+__host__ __device__ constexpr int lag_table_ints(int ntau, int nunion, int ngroups, int nruns) {
+    return kTabEntries + 3 * ntau + nunion + ngroups + 1 + nruns;
+}
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -119,26 +141,46 @@ __device__ __forceinline__ float f2_hsum(unsigned long long v) {
     return __uint_as_float(static_cast<unsigned>(v)) + __uint_as_float(static_cast<unsigned>(v >> 32));
 }
 
-// Warp-specialised pipeline. Warps 0..kLagConsumerWarps-1 consume (one spectrum element
-// per thread); the last warp produces (its lane 0 issues the bulk copies). Per ring slot,
-// full[slot] completes when the slot's frame has landed and empty[slot] when every consumer
-// warp has released it, so neither side ever waits for the whole CTA.
+// 2-D TMA copy of a box of `rows` consecutive ring slots x kLagBlock elements (the box
+// shape is fixed by the tensor map) into shared memory, completing on `bar`.
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Tensor maps of the ring viewed as a 2-D array [slots][elements] of 8-byte values, with
+// boxes of kLagBlock elements x 1, 2, 4 or 8 slots.
+struct LagMaps {
+    CUtensorMap box[kLagRunKinds];
+};
+
+// Warp-specialised pipeline over groups of kLagGroup union entries. Warps
+// 0..kLagConsumerWarps-1 consume (one spectrum element per thread); the last warp produces
+// (its lane 0 issues the copies). Group g occupies shared-memory slots
+// [(g % groups) * kLagGroup, +kLagGroup); its consecutive ring slots arrive as a few 2-D
+// boxes (runs) that all complete on full[g % groups]; empty[g % groups] completes when every
+// consumer warp has moved past the group. Neither side ever waits for the whole CTA.
 template <int J>
 __global__ void __launch_bounds__(kLagThreads, 3)
     lag_pipe_kernel(const float2 *__restrict__ ring, float2 *__restrict__ acc, long long E,
-                    const int *__restrict__ table, int *__restrict__ status) {
-    extern __shared__ __align__(1024) unsigned char smem[];
+                    const int *__restrict__ table, int *__restrict__ status, const __grid_constant__ LagMaps maps) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // ring slots must start on 1 KB boundaries (TMA destinations): align the base at run time
+    unsigned char *smem = smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u);
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + kLagRingBytes);
-    uint64_t *empty = full + kLagSlots;
-    volatile int *abort_flag = reinterpret_cast<volatile int *>(empty + kLagSlots);
+    uint64_t *empty = full + kLagGroupSlots;
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(empty + kLagGroupSlots);
     int *tab = const_cast<int *>(reinterpret_cast<volatile int *>(abort_flag + 1));
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-    const int ntab = kTabEntries + 3 * table[kTabNtau] + table[kTabNunion];
+    const int ntab = lag_table_ints(table[kTabNtau], table[kTabNunion], table[kTabNgroups], table[kTabNruns]);
     for (int i = tid; i < ntab; i += kLagThreads) tab[i] = table[i];
     if (tid == 0) {
-        for (int i = 0; i < kLagSlots; i++) {
+        for (int i = 0; i < kLagGroupSlots; i++) {
             mbar_init(&full[i], 1);
             mbar_init(&empty[i], kLagConsumerWarps);
         }
@@ -148,31 +190,38 @@ __global__ void __launch_bounds__(kLagThreads, 3)
     __syncthreads();
 
     const int nreg = tab[kTabNreg], ntau = tab[kTabNtau], nu = tab[kTabNunion];
+    const int ngroups = tab[kTabNgroups];
     const int *ent_acc = tab + kTabEntries;
     const int *ent_ub = ent_acc + ntau;
     const int *ent_full = ent_ub + ntau;
     const int *uslot = ent_full + ntau;
+    const int *gptr = uslot + nu;
+    const int *runs = gptr + ngroups + 1;
     const long long e0 = static_cast<long long>(blockIdx.x) * kLagBlock;
 
     if (warp == kLagConsumerWarps) {
-        // ---------------- producer: union index u is fill u / kLagSlots of slot u % kLagSlots
+        // ---------------- producer: group g is fill g / kLagGroupSlots of group slot g % kLagGroupSlots
         if (lane == 0) {
-            const uint32_t bytes = static_cast<uint32_t>(
-                sizeof(float2) * (E - e0 < kLagBlock ? E - e0 : static_cast<long long>(kLagBlock)));
-            for (int u = 0; u < nu; u++) {
-                const int slot = u & (kLagSlots - 1), fill = u >> kLagSlotsLog2;
-                if (fill > 0 && !mbar_wait_bounded(&empty[slot], (fill - 1) & 1)) {
+            for (int g = 0; g < ngroups; g++) {
+                const int gs = g & (kLagGroupSlots - 1), fill = g >> kLagGroupSlotsLog2;
+                if (fill > 0 && !mbar_wait_bounded(&empty[gs], (fill - 1) & 1)) {
                     *abort_flag = 1;
                     break;
                 }
                 if (*abort_flag) break;
-                const int s = uslot[u];
-                if (s < 0) {  // no such frame: complete the phase without data, nobody reads it
-                    mbar_arrive(&full[slot]);
+                const int r0 = gptr[g], r1 = gptr[g + 1];
+                if (r0 == r1) {  // no frame in the group: complete the phase without data
+                    mbar_arrive(&full[gs]);
                     continue;
                 }
-                mbar_expect_tx(&full[slot], bytes);
-                bulk_load(smem + slot * kLagSlotBytes, ring + static_cast<long long>(s) * E + e0, bytes, &full[slot]);
+                uint32_t bytes = 0;
+                for (int r = r0; r < r1; r++) bytes += kLagSlotBytes << lag_run_log2rows(runs[r]);
+                mbar_expect_tx(&full[gs], bytes);
+                for (int r = r0; r < r1; r++) {
+                    const int run = runs[r];
+                    tma_load_2d(smem + (gs * kLagGroup + lag_run_rel(run)) * kLagSlotBytes,
+                                &maps.box[lag_run_log2rows(run)], static_cast<int>(e0), lag_run_slot(run), &full[gs]);
+                }
             }
         }
     } else {
@@ -191,22 +240,22 @@ __global__ void __launch_bounds__(kLagThreads, 3)
         float2 a0 = (valid && ntau > 0) ? acc[static_cast<long long>(ent_acc[0]) * E + k] : zero;
         float2 a1 = (valid && ntau > 1) ? acc[static_cast<long long>(ent_acc[1]) * E + k] : zero;
         float2 a2 = (valid && ntau > 2) ? acc[static_cast<long long>(ent_acc[2]) * E + k] : zero;
-        int waited = 0, released = 0;
+        int waited = 0, released = 0;  // in groups
         for (int e = 0; e < ntau; e++) {
             const float2 a3 = (valid && e + 3 < ntau) ? acc[static_cast<long long>(ent_acc[e + 3]) * E + k] : zero;
             const int ub = ent_ub[e];
+            // Wait for every group this window reaches that no earlier window reached; groups
+            // without frames included (they complete by the producer's bare arrival), so a
+            // consumer never releases a group the producer has not issued yet.
+            const int glast = (ub + nreg - 1) >> kLagGroupLog2;
             bool ok = true;
-            // Wait for the entries new to this window, those without a frame included (the
-            // producer's bare arrival): a consumer must never release a fill of a slot that
-            // the producer has not issued yet, or the slot's empty barrier would run a phase
-            // ahead of the producer's parity.
-            for (int u = waited > ub ? waited : ub; u < ub + nreg; u++) {
-                if (!mbar_wait_bounded(&full[u & (kLagSlots - 1)], (u >> kLagSlotsLog2) & 1)) {
+            for (int g = waited; g <= glast; g++) {
+                if (!mbar_wait_bounded(&full[g & (kLagGroupSlots - 1)], (g >> kLagGroupSlotsLog2) & 1)) {
                     ok = false;
                     break;
                 }
             }
-            waited = ub + nreg;
+            if (glast + 1 > waited) waited = glast + 1;
             if (!ok) *abort_flag = 1;
             if (*abort_flag) break;
             const uint32_t o = static_cast<uint32_t>(ub) * kLagSlotBytes;
@@ -238,11 +287,11 @@ __global__ void __launch_bounds__(kLagThreads, 3)
             a0 = a1;
             a1 = a2;
             a2 = a3;
-            // release the slots no later entry reads
-            const int next = e + 1 < ntau ? ent_ub[e + 1] : nu;
+            // release the groups no later window reads (all their entries lie below the next window)
+            const int next_g = (e + 1 < ntau ? ent_ub[e + 1] : nu) >> kLagGroupLog2;
             __syncwarp();
             if (lane == 0)
-                for (; released < next; released++) mbar_arrive(&empty[released & (kLagSlots - 1)]);
+                for (; released < next_g; released++) mbar_arrive(&empty[released & (kLagGroupSlots - 1)]);
         }
     }
     __syncthreads();
@@ -250,10 +299,10 @@ __global__ void __launch_bounds__(kLagThreads, 3)
         if (tid == 0) {
             atomicExch(status, 1);
             // drain: wait (bounded) until every copy this CTA issued has landed
-            for (int slot = 0; slot < kLagSlots; slot++) {
-                for (int u = slot; u < nu; u += kLagSlots) {
-                    if (uslot[u] >= 0 && !mbar_try_wait(&full[slot], (u >> kLagSlotsLog2) & 1)) {
-                        mbar_wait_bounded(&full[slot], (u >> kLagSlotsLog2) & 1);
+            for (int gs = 0; gs < kLagGroupSlots; gs++) {
+                for (int g = gs; g < ngroups; g += kLagGroupSlots) {
+                    if (!mbar_try_wait(&full[gs], (g >> kLagGroupSlotsLog2) & 1)) {
+                        mbar_wait_bounded(&full[gs], (g >> kLagGroupSlotsLog2) & 1);
                         break;
                     }
                 }
@@ -264,7 +313,7 @@ __global__ void __launch_bounds__(kLagThreads, 3)
 }
 
 inline size_t lag_smem_bytes(int table_ints) {
-    return kLagRingBytes + 2 * sizeof(uint64_t) * kLagSlots + sizeof(int) * (1 + table_ints);
+    return 1024 + kLagRingBytes + 2 * sizeof(uint64_t) * kLagGroupSlots + sizeof(int) * (1 + table_ints);
 }
 
 }  // namespace ddm
