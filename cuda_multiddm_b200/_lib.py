@@ -72,6 +72,8 @@ SIGNATURES = {
     "ddm_build_masks": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_float, C.c_void_p, C.c_void_p]),
     "ddm_compat_schedule": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ddm_lag_accumulate_static": (C.c_int, [C.c_void_p, C.c_int, C.c_longlong, C.c_void_p, C.c_void_p, C.c_int,
+                                            C.c_void_p, C.c_int, C.c_void_p]),
     "ddm_host_alloc": (C.c_void_p, [C.c_size_t]),
     "ddm_host_free": (None, [C.c_void_p]),
     "ddm_last_error": (C.c_char_p, []),

@@ -173,6 +173,27 @@ int ddm_compat_schedule(int total_frames, int chunk, int multistream, int dump_e
                         int tau_count, int max_calls, int *a_out, int *b_out, int *epoch_out,
                         int *frames_read);
 
+/* Lag accumulation on caller-owned device memory, with no device allocation at all. This
+ * entry point has no counterpart in the reference. It exists for callers that cannot let a
+ * library call cudaMalloc -- real-time acquisition loops that reserve all device memory at
+ * start-up and must not stall mid-stream, and applications whose own pool allocator owns
+ * every device buffer. For every element k < elements and tau row t < tau_count:
+ *   acc[t][k] += sum over j < frame_count of |ring[a_slots[j]][k] - ring[b_slots[t*frame_count + j]][k]|^2
+ * skipping pairs with a slot of -1; ring is float2[ring_slots][elements] (complex spectra,
+ * elements even), acc is float2[tau_count][elements] holding {sum, Kahan compensation}
+ * (value = sum - compensation), both device pointers on the current device; the engine's
+ * lag kernel does the work, on `stream` (a cudaStream_t, NULL = default stream).
+ * Limits: frame_count <= 32, tau_count <= 128, ring_slots <= 1048575; larger requests are
+ * refused with DDM_ERR_INVALID_ARG. The kernel's pair table and status word live in one
+ * static device array of about 37 KB that every GPU using the library keeps until exit and
+ * that all calls share: calls are serialised in the process and each returns after its
+ * kernel finished; kernels of calls made from other processes do not share it. The first
+ * call on each device sets that device up (cudaGetSymbolAddress of the array and the
+ * kernel's shared-memory limit), so make the first call before any stream capture. */
+int ddm_lag_accumulate_static(const void *ring, int ring_slots, long long elements, void *acc,
+                              const int *a_slots, int frame_count, const int *b_slots, int tau_count,
+                              void *stream);
+
 /* Page-locked host memory for frame buffers (asynchronous copies); NULL on failure. */
 void *ddm_host_alloc(size_t bytes);
 void ddm_host_free(void *ptr);
