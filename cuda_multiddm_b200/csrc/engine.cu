@@ -196,7 +196,6 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
     rows.E = e->E;
     rows.R = e->R;
     rows.tw = e->tw;
-    rows.log2M = log2i(e->M);
     cols = rows;
     int row_ctas = 0, col_ctas = 0;
     size_t smem = 0;
@@ -207,6 +206,7 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
         fs.s = s;
         fs.log2s = log2i(s);
         fs.tiles_side = side;
+        fs.log2side = log2i(side);
         fs.n = d.n;
         fs.off = d.off;
         fs.cta_begin = row_ctas;
@@ -566,14 +566,9 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
         if (cudaEventCreateWithFlags(&e->tab_ev[i], cudaEventDisableTiming) != cudaSuccess)
             return bail(fail(DDM_ERR_CUDA, "cudaEventCreate failed"));
 
-    // Twiddles e^{-2 pi i m / M}, m < M, from FP64 math rounded to FP32
+    // FFT twiddle tables (FP64 math rounded to FP32), one per transform length
     {
-        std::vector<float2> tw(e->M);
-        const double two_pi = 6.283185307179586476925286766559;
-        for (int m = 0; m < e->M; m++) {
-            double a = two_pi * m / e->M;
-            tw[m] = make_float2(static_cast<float>(std::cos(a)), static_cast<float>(-std::sin(a)));
-        }
+        std::vector<float2> tw = fft_twiddle_tables(e->M);
         if ((st = dev_alloc(e, &e->tw, tw.size()))) return bail(st);
         if (cudaMemcpy(e->tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice) != cudaSuccess)
             return bail(fail(DDM_ERR_CUDA, "twiddle upload failed"));

@@ -19,11 +19,16 @@
 // at i + i/16 (one float2 of padding per 16) so the strided stores of a pass hit distinct
 // banks; transforms are kFftPad(L) elements apart.
 //
-// Twiddles e^{-2 pi i m / M} (M = largest scale) come from a table computed in FP64 on the
-// host and rounded to FP32; the radix-16 kernels use the exact values of cos/sin(k pi/8).
+// Every transform length is a template parameter (one instance per log2 L, chosen per scale
+// at run time), so all index arithmetic folds to constants. Twiddles come from per-length
+// tables computed in FP64 on the host and rounded to FP32; the radix-16 kernels use the
+// exact values of cos/sin(k pi/8).
 #pragma once
 
+#include <cmath>
 #include <cstdint>
+#include <vector>
+
 #include <cuda_runtime.h>
 
 namespace ddm {
@@ -122,71 +127,65 @@ __device__ __forceinline__ void dft_reg(float2 *v) {
 template <int R>
 __host__ __device__ constexpr int ilog2c() { return R <= 1 ? 0 : 1 + ilog2c<R / 2>(); }
 
-// One Stockham pass of radix R over a transform of length L at buf (padded layout), by
-// thread t of a team of `team`; every thread handles 16/R groups (R = L for L < 16).
-template <int R>
-__device__ __forceinline__ void stockham_pass(float2 *buf, int L, int Ns, int t, int team,
-                                              const float2 *__restrict__ tw, int log2M, bool active) {
-    constexpr int G = R >= 16 ? 1 : 16 / R;
+// One Stockham pass of radix R over a transform of length L = 2^LOG2L held in buf (padded
+// layout) by thread t of its team, with NS the product of the earlier passes' radices.
+// Every thread handles G = STRIDE/TEAM groups of R values (1 group for radix 16).
+// tw is the table of length L: tw[m] = e^{-2 pi i m / L}.
+template <int LOG2L, int R, int NS>
+__device__ __forceinline__ void stockham_pass(float2 *buf, int t, const float2 *__restrict__ tw) {
+    constexpr int L = 1 << LOG2L;
+    constexpr int TEAM = L >= 16 ? L / 16 : 1;
+    constexpr int STRIDE = L / R;
+    constexpr int G = STRIDE / TEAM < 1 ? 1 : STRIDE / TEAM;
+    constexpr int SHIFT = LOG2L - ilog2c<NS>() - ilog2c<R>();  // e^{-2 pi i jm r / (NS R)} = tw[(jm r) << SHIFT]
     float2 v[G * R];
-    const int stride = L / R;
-    int ngroups = stride / team;  // groups per thread (1 for radix 16)
-    if (ngroups > G) ngroups = G;
-    if (active) {
 #pragma unroll
-        for (int g = 0; g < G; g++) {
-            if (g < ngroups) {
-                const int j = t + g * team;
-                const int jm = j & (Ns - 1);
+    for (int g = 0; g < G; g++) {
+        const int j = t + g * TEAM;
+        const int jm = j & (NS - 1);
 #pragma unroll
-                for (int r = 0; r < R; r++) {
-                    float2 x = buf[fpad(j + r * stride)];
-                    if (r > 0 && Ns > 1) {
-                        // e^{-2 pi i (j mod Ns) r / (Ns R)} = tw[(j mod Ns) r M / (Ns R)]
-                        const int m = (jm * r) << (log2M - (__ffs(Ns) - 1) - ilog2c<R>());
-                        x = cmulf(x, __ldg(tw + m));
-                    }
-                    v[g * R + r] = x;
-                }
-            }
+        for (int r = 0; r < R; r++) {
+            float2 x = buf[fpad(j + r * STRIDE)];
+            if (NS > 1 && r > 0) x = cmulf(x, __ldg(tw + ((jm * r) << SHIFT)));
+            v[g * R + r] = x;
         }
     }
     __syncthreads();
-    if (active) {
 #pragma unroll
-        for (int g = 0; g < G; g++) {
-            if (g < ngroups) {
-                dft_reg<R>(v + g * R);
-                const int j = t + g * team;
-                const int idx = (j & ~(Ns - 1)) * R + (j & (Ns - 1));
+    for (int g = 0; g < G; g++) {
+        dft_reg<R>(v + g * R);
+        const int j = t + g * TEAM;
+        const int idx = (j & ~(NS - 1)) * R + (j & (NS - 1));
 #pragma unroll
-                for (int r = 0; r < R; r++) buf[fpad(idx + r * Ns)] = v[g * R + r];
-            }
-        }
+        for (int r = 0; r < R; r++) buf[fpad(idx + r * NS)] = v[g * R + r];
     }
     __syncthreads();
 }
 
-// Full forward transform of length L (= 2^log2L <= 2^kFftMaxLog2) of the team's buffer.
-__device__ void fft_team_transform(float2 *buf, int log2L, int t, int team, const float2 *__restrict__ tw,
-                                   int log2M, bool active) {
-    const int L = 1 << log2L;
-    if (L < 16) {
-        if (L == 2) stockham_pass<2>(buf, L, 1, t, team, tw, log2M, active);
-        else if (L == 4) stockham_pass<4>(buf, L, 1, t, team, tw, log2M, active);
-        else if (L == 8) stockham_pass<8>(buf, L, 1, t, team, tw, log2M, active);
-        return;
+// Forward transform of length 2^LOG2L: radix-16 passes, then one pass of radix 2, 4 or 8.
+template <int LOG2L, int NS = 1>
+__device__ __forceinline__ void fft_transform(float2 *buf, int t, const float2 *__restrict__ tw) {
+    constexpr int L = 1 << LOG2L;
+    if constexpr (L < 16) {
+        stockham_pass<LOG2L, L, 1>(buf, t, tw);
+    } else {
+        constexpr int left = LOG2L - ilog2c<NS>();
+        if constexpr (left >= 4) {
+            stockham_pass<LOG2L, 16, NS>(buf, t, tw);
+            fft_transform<LOG2L, NS * 16>(buf, t, tw);
+        } else if constexpr (left == 3) {
+            stockham_pass<LOG2L, 8, NS>(buf, t, tw);
+        } else if constexpr (left == 2) {
+            stockham_pass<LOG2L, 4, NS>(buf, t, tw);
+        } else if constexpr (left == 1) {
+            stockham_pass<LOG2L, 2, NS>(buf, t, tw);
+        }
     }
-    int Ns = 1, left = log2L;
-    for (; left >= 4; left -= 4, Ns <<= 4) stockham_pass<16>(buf, L, Ns, t, team, tw, log2M, active);
-    if (left == 1) stockham_pass<2>(buf, L, Ns, t, team, tw, log2M, active);
-    else if (left == 2) stockham_pass<4>(buf, L, Ns, t, team, tw, log2M, active);
-    else if (left == 3) stockham_pass<8>(buf, L, Ns, t, team, tw, log2M, active);
 }
 
 // Per-scale launch geometry shared by both passes (ctas_per_frame over row pairs or columns).
 struct FftScale {
-    int s, log2s, tiles_side;
+    int s, log2s, tiles_side, log2side;
     int ctas_per_frame;
     int cta_begin;        // first CTA (blockIdx.x) of this scale
     long long n, off;     // elements per tile, offset of the scale in a frame
@@ -204,8 +203,7 @@ struct FftArgs {
     long long E;
     long long first_label;
     int R;
-    const float2 *tw;
-    int log2M;
+    const float2 *tw;  // tables of length 2, 4, ..., M back to back: the one of length L at tw + L - 2
 };
 
 __device__ __forceinline__ int fft_find_scale(const FftArgs &a) {
@@ -219,85 +217,137 @@ __device__ __forceinline__ float fft_pixel(const uint8_t *p, int pixmode) {
     return static_cast<float>(p[0]);
 }
 
-// grid (sum of ctas_per_frame, frames). CTA = fft_per_cta(s) consecutive row pairs of the
-// flattened (tile, pair) index of one frame at one scale.
-__global__ void __launch_bounds__(kFftThreads) fft_rows_kernel(FftArgs a) {
-    extern __shared__ float2 fsm[];
-    const FftScale &sc = a.sc[fft_find_scale(a)];
-    const int s = sc.s, L = s, team = fft_team(L), nT = fft_per_cta(L), TS = kFftPad(L);
-    const int pairs_per_tile = s / 2;
-    const int total_pairs = sc.tiles_side * sc.tiles_side * pairs_per_tile;
-    const int g0 = (blockIdx.x - sc.cta_begin) * nT;
-    const int f = blockIdx.y;
-    const uint8_t *fsrc = a.src + f * a.frame_stride;
-    // load: element (c, i) = (pixel(row 2p, i), pixel(row 2p+1, i)) of pair g0 + c
-    for (int q = threadIdx.x; q < nT * L; q += kFftThreads) {
-        const int c = q >> sc.log2s, i = q & (L - 1);
+// Row pass at scale 2^LOG2L: the CTA transforms NT consecutive row pairs of the flattened
+// (tile, pair) index of frame blockIdx.y, rows 2p and 2p+1 packed as real and imaginary parts.
+template <int LOG2L>
+__device__ __forceinline__ void fft_rows_body(const FftArgs &a, const FftScale &sc, float2 *fsm) {
+    constexpr int L = 1 << LOG2L, TEAM = fft_team(L), NT = fft_per_cta(L), TS = kFftPad(L);
+    constexpr int NX = L / 2 + 1;
+    constexpr int ITER = NT * L / kFftThreads;
+    const int total_pairs = (1 << (2 * sc.log2side)) * (L / 2);
+    const int g0 = (blockIdx.x - sc.cta_begin) * NT;
+    const uint8_t *fsrc = a.src + blockIdx.y * a.frame_stride;
+#pragma unroll 4
+    for (int it = 0; it < ITER; it++) {
+        const int q = threadIdx.x + it * kFftThreads;
+        const int c = q >> LOG2L, i = q & (L - 1);
         const int g = g0 + c;
         float2 z = make_float2(0.f, 0.f);
         if (g < total_pairs) {
-            const int tile = g / pairs_per_tile, py = 2 * (g - tile * pairs_per_tile);
-            const int ty = tile / sc.tiles_side, tx = tile - ty * sc.tiles_side;
-            const long long Y = static_cast<long long>(ty) * s + py + a.y_off;
-            const long long X = static_cast<long long>(tx) * s + i + a.x_off;
+            const int tile = g >> (LOG2L - 1 > 0 ? LOG2L - 1 : 0);
+            const int py = 2 * (g & (L / 2 - 1));
+            const int ty = tile >> sc.log2side, tx = tile & (sc.tiles_side - 1);
+            const long long Y = (static_cast<long long>(ty) << LOG2L) + py + a.y_off;
+            const long long X = (static_cast<long long>(tx) << LOG2L) + i + a.x_off;
             const uint8_t *p0 = fsrc + Y * a.row_pitch + X * a.bpp;
             z = make_float2(fft_pixel(p0, a.pixmode), fft_pixel(p0 + a.row_pitch, a.pixmode));
         }
         fsm[c * TS + fpad(i)] = z;
     }
     __syncthreads();
-    const int c_me = threadIdx.x / team, t = threadIdx.x - c_me * team;
-    fft_team_transform(fsm + c_me * TS, sc.log2s, t, team, a.tw, a.log2M, c_me < nT);
+    const int c_me = threadIdx.x / TEAM, t = threadIdx.x & (TEAM - 1);
+    float2 *buf = fsm + c_me * TS;
+    fft_transform<LOG2L>(buf, t, a.tw + (L - 2));
     // split Z = X0 + i X1 into the two real rows' half spectra
-    const int nx = s / 2 + 1;
-    const long long slot = (a.first_label + f) % a.R;
-    float2 *out = a.ring + slot * a.E + sc.off;
-    for (int q = threadIdx.x; q < nT * nx; q += kFftThreads) {
-        const int c = q / nx, k = q - c * nx;
-        const int g = g0 + c;
-        if (g >= total_pairs) continue;
-        const float2 *z = fsm + c * TS;
-        const float2 zk = z[fpad(k & (L - 1))], zm = z[fpad((L - k) & (L - 1))];
-        const int tile = g / pairs_per_tile, py = 2 * (g - tile * pairs_per_tile);
-        float2 *o = out + tile * sc.n + static_cast<long long>(py) * nx + k;
-        o[0] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
-        o[nx] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+    const int g = g0 + c_me;
+    if (g >= total_pairs) return;
+    const int tile = g >> (LOG2L - 1 > 0 ? LOG2L - 1 : 0);
+    const int py = 2 * (g & (L / 2 - 1));
+    const long long slot = (a.first_label + blockIdx.y) % a.R;
+    float2 *o = a.ring + slot * a.E + sc.off + tile * sc.n + static_cast<long long>(py) * NX;
+#pragma unroll
+    for (int m = 0; m < (NX + TEAM - 1) / TEAM; m++) {
+        const int k = t + m * TEAM;
+        if (k < NX) {
+            const float2 zk = buf[fpad(k & (L - 1))], zm = buf[fpad((L - k) & (L - 1))];
+            o[k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+            o[NX + k] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+        }
     }
 }
 
-// grid (sum of ctas_per_frame, frames). CTA = fft_per_cta(s) consecutive columns of the
-// flattened (tile, kx) index of one frame at one scale, transformed along y in place.
-__global__ void __launch_bounds__(kFftThreads) fft_cols_kernel(FftArgs a) {
-    extern __shared__ float2 fsm[];
-    const FftScale &sc = a.sc[fft_find_scale(a)];
-    const int s = sc.s, L = s, team = fft_team(L), nT = fft_per_cta(L), TS = kFftPad(L);
-    const int nx = s / 2 + 1;
-    const int total_cols = sc.tiles_side * sc.tiles_side * nx;
-    const int g0 = (blockIdx.x - sc.cta_begin) * nT;
+// Column pass at scale 2^LOG2L: NT consecutive columns of the flattened (tile, kx) index of
+// frame blockIdx.y, transformed along y in place.
+template <int LOG2L>
+__device__ __forceinline__ void fft_cols_body(const FftArgs &a, const FftScale &sc, float2 *fsm) {
+    constexpr int L = 1 << LOG2L, TEAM = fft_team(L), NT = fft_per_cta(L), TS = kFftPad(L);
+    constexpr int NX = L / 2 + 1;
+    constexpr int LOG2NT = ilog2c<NT>();
+    constexpr int ITER = NT * L / kFftThreads;
+    const int total_cols = (1 << (2 * sc.log2side)) * NX;
+    const int g0 = (blockIdx.x - sc.cta_begin) * NT;
     const long long slot = (a.first_label + blockIdx.y) % a.R;
     float2 *base = a.ring + slot * a.E + sc.off;
-    for (int q = threadIdx.x; q < nT * L; q += kFftThreads) {
-        const int y = q / nT, c = q - y * nT;
+#pragma unroll 4
+    for (int it = 0; it < ITER; it++) {
+        const int q = threadIdx.x + it * kFftThreads;
+        const int y = q >> LOG2NT, c = q & (NT - 1);
         const int g = g0 + c;
         float2 v = make_float2(0.f, 0.f);
         if (g < total_cols) {
-            const int tile = g / nx, col = g - tile * nx;
-            v = base[tile * sc.n + static_cast<long long>(y) * nx + col];
+            const int tile = g / NX, col = g - tile * NX;
+            v = base[tile * sc.n + static_cast<long long>(y) * NX + col];
         }
         fsm[c * TS + fpad(y)] = v;
     }
     __syncthreads();
-    const int c_me = threadIdx.x / team, t = threadIdx.x - c_me * team;
-    fft_team_transform(fsm + c_me * TS, sc.log2s, t, team, a.tw, a.log2M, c_me < nT);
-    for (int q = threadIdx.x; q < nT * L; q += kFftThreads) {
-        const int y = q / nT, c = q - y * nT;
+    const int c_me = threadIdx.x / TEAM, t = threadIdx.x & (TEAM - 1);
+    fft_transform<LOG2L>(fsm + c_me * TS, t, a.tw + (L - 2));
+#pragma unroll 4
+    for (int it = 0; it < ITER; it++) {
+        const int q = threadIdx.x + it * kFftThreads;
+        const int y = q >> LOG2NT, c = q & (NT - 1);
         const int g = g0 + c;
-        if (g >= total_cols) continue;
-        const int tile = g / nx, col = g - tile * nx;
-        base[tile * sc.n + static_cast<long long>(y) * nx + col] = fsm[c * TS + fpad(y)];
+        if (g < total_cols) {
+            const int tile = g / NX, col = g - tile * NX;
+            base[tile * sc.n + static_cast<long long>(y) * NX + col] = fsm[c * TS + fpad(y)];
+        }
     }
 }
 
+#define DDM_FFT_DISPATCH(BODY)                      \
+    switch (sc.log2s) {                             \
+        case 1: BODY<1>(a, sc, fsm); break;         \
+        case 2: BODY<2>(a, sc, fsm); break;         \
+        case 3: BODY<3>(a, sc, fsm); break;         \
+        case 4: BODY<4>(a, sc, fsm); break;         \
+        case 5: BODY<5>(a, sc, fsm); break;         \
+        case 6: BODY<6>(a, sc, fsm); break;         \
+        case 7: BODY<7>(a, sc, fsm); break;         \
+        case 8: BODY<8>(a, sc, fsm); break;         \
+        case 9: BODY<9>(a, sc, fsm); break;         \
+        case 10: BODY<10>(a, sc, fsm); break;       \
+        case 11: BODY<11>(a, sc, fsm); break;       \
+        default: BODY<12>(a, sc, fsm); break;       \
+    }
+
+// grid (sum of ctas_per_frame, frames)
+__global__ void __launch_bounds__(kFftThreads) fft_rows_kernel(FftArgs a) {
+    extern __shared__ float2 fsm[];
+    const FftScale &sc = a.sc[fft_find_scale(a)];
+    DDM_FFT_DISPATCH(fft_rows_body)
+}
+
+__global__ void __launch_bounds__(kFftThreads) fft_cols_kernel(FftArgs a) {
+    extern __shared__ float2 fsm[];
+    const FftScale &sc = a.sc[fft_find_scale(a)];
+    DDM_FFT_DISPATCH(fft_cols_body)
+}
+#undef DDM_FFT_DISPATCH
+
 inline size_t fft_smem_bytes(int L) { return sizeof(float2) * static_cast<size_t>(fft_per_cta(L)) * kFftPad(L); }
+
+// Twiddle tables for lengths 2, 4, ..., M back to back (length L at offset L - 2), from FP64
+// math rounded to FP32: entry m of the length-L table is e^{-2 pi i m / L}.
+inline std::vector<float2> fft_twiddle_tables(int M) {
+    std::vector<float2> tw;
+    const double two_pi = 6.283185307179586476925286766559;
+    for (int L = 2; L <= M; L <<= 1)
+        for (int m = 0; m < L; m++) {
+            const double ang = two_pi * m / L;
+            tw.push_back(make_float2(static_cast<float>(std::cos(ang)), static_cast<float>(-std::sin(ang))));
+        }
+    return tw;
+}
 
 }  // namespace ddm
