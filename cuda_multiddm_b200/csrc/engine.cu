@@ -75,8 +75,17 @@ struct ddm_engine {
     long long isf_size = 0;
 
     // device state
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;      // lag, azimuth, accumulator work ("main")
     bool own_stream = false;
+    // The FFT of a piece runs on its own stream, so it overlaps the lag kernel of the piece
+    // before (the FFT is compute/L2-bound, the lag kernel HBM-bound). ev_fft orders each lag
+    // after the FFT of its frames; ev_guard[piece & 1], recorded on the main stream when a
+    // piece's FFT is issued, holds back the next piece's FFT until every lag issued before
+    // this one has finished, so an FFT never overwrites ring slots a running lag still reads
+    // (the ring carries one extra piece of slots for that).
+    cudaStream_t fft_stream = nullptr;
+    cudaEvent_t ev_fft = nullptr, ev_guard[2] = {nullptr, nullptr};
+    long long pieces = 0;
     int R = 0, jmax = 32;
     float2 *ring = nullptr, *acc = nullptr, *tw = nullptr;
     uint8_t *stage = nullptr;
@@ -150,6 +159,10 @@ void free_all(ddm_engine *e) {
             cudaEventDestroy(pr.first);
             cudaEventDestroy(pr.second);
         }
+    if (e->ev_fft) cudaEventDestroy(e->ev_fft);
+    for (cudaEvent_t ev : e->ev_guard)
+        if (ev) cudaEventDestroy(ev);
+    if (e->fft_stream) cudaStreamDestroy(e->fft_stream);
     if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
 }
 
@@ -157,16 +170,17 @@ void free_all(ddm_engine *e) {
 struct TimedRange {
     ddm_engine *e;
     int group;
+    cudaStream_t stream;
     cudaEvent_t start = nullptr;
-    TimedRange(ddm_engine *e_, int g) : e(e_), group(g) {
-        if (e->timing && cudaEventCreate(&start) == cudaSuccess) cudaEventRecord(start, e->stream);
+    TimedRange(ddm_engine *e_, int g) : e(e_), group(g), stream(g == 0 ? e_->fft_stream : e_->stream) {
+        if (e->timing && cudaEventCreate(&start) == cudaSuccess) cudaEventRecord(start, stream);
     }
     void end(long launches) {
         e->tlaunch[group] += launches;
         if (!start) return;
         cudaEvent_t stop;
         if (cudaEventCreate(&stop) == cudaSuccess) {
-            cudaEventRecord(stop, e->stream);
+            cudaEventRecord(stop, stream);
             e->tev[group].push_back({start, stop});
         } else {
             cudaEventDestroy(start);
@@ -227,9 +241,9 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
         const int nf = std::min(group, nframes - f0);
         rows.src = src + f0 * frame_stride;
         rows.first_label = cols.first_label = first_label + f0;
-        fft_rows_kernel<<<dim3(row_ctas, nf), kFftThreads, smem, e->stream>>>(rows);
+        fft_rows_kernel<<<dim3(row_ctas, nf), kFftThreads, smem, e->fft_stream>>>(rows);
         CUDA_TRY(cudaGetLastError());
-        fft_cols_kernel<<<dim3(col_ctas, nf), kFftThreads, smem, e->stream>>>(cols);
+        fft_cols_kernel<<<dim3(col_ctas, nf), kFftThreads, smem, e->fft_stream>>>(cols);
         CUDA_TRY(cudaGetLastError());
         e->launches += 2;
         tr.e->tlaunch[0] += 2;
@@ -513,9 +527,9 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
             run = std::max(run, it.max_label);
             if (it.max_label >= 0) span = std::max(span, run + e->jmax - it.min_label + 1);
         }
-        e->R = span;
+        e->R = span + e->jmax;  // + one piece: the next piece's FFT overlaps the running lag
     } else {
-        e->R = e->tau_max + e->jmax;
+        e->R = e->tau_max + 2 * e->jmax;  // window of one piece + one piece of FFT overlap
         e->pair_count.assign(e->T, 0.0);
     }
 
@@ -546,6 +560,11 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
             return bail(fail(DDM_ERR_CUDA, "cudaStreamCreate failed"));
         e->own_stream = true;
     }
+    if (cudaStreamCreateWithFlags(&e->fft_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e->ev_fft, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e->ev_guard[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e->ev_guard[1], cudaEventDisableTiming) != cudaSuccess)
+        return bail(fail(DDM_ERR_CUDA, "stream/event creation failed"));
     int st;
     if ((st = dev_alloc(e, &e->ring, static_cast<size_t>(e->R) * e->E))) return bail(st);
     {
@@ -618,6 +637,7 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
 
 extern "C" int ddm_close(ddm_engine *e) {
     if (!e) return DDM_OK;
+    if (e->fft_stream) cudaStreamSynchronize(e->fft_stream);
     if (e->stream) cudaStreamSynchronize(e->stream);
     free_all(e);
     delete e;
@@ -643,6 +663,10 @@ extern "C" int ddm_submit_frames(ddm_engine *e, const void *frames, int count, i
         }
         const uint8_t *p = src + frame_bytes * done;
         int st;
+        // hold this piece's FFT until every lag issued before the previous piece's FFT is done
+        if (e->pieces > 0) CUDA_TRY(cudaStreamWaitEvent(e->fft_stream, e->ev_guard[(e->pieces - 1) & 1], 0));
+        CUDA_TRY(cudaEventRecord(e->ev_guard[e->pieces & 1], e->stream));
+        e->pieces++;
         if (on_device) {
             st = launch_fft(e, p, static_cast<long long>(frame_bytes), static_cast<long long>(e->w) * e->bpp,
                             e->x_off, e->y_off, piece, e->submitted);
@@ -653,12 +677,14 @@ extern "C" int ddm_submit_frames(ddm_engine *e, const void *frames, int count, i
                                     (static_cast<size_t>(e->y_off) * e->w + e->x_off) * e->bpp;
                 CUDA_TRY(cudaMemcpy2DAsync(e->stage + static_cast<size_t>(f) * e->M * roi_row, roi_row, fp,
                                            static_cast<size_t>(e->w) * e->bpp, roi_row, e->M,
-                                           cudaMemcpyHostToDevice, e->stream));
+                                           cudaMemcpyHostToDevice, e->fft_stream));
             }
             st = launch_fft(e, e->stage, static_cast<long long>(e->M) * roi_row, static_cast<long long>(roi_row),
                             0, 0, piece, e->submitted);
         }
         if (st) return st;
+        CUDA_TRY(cudaEventRecord(e->ev_fft, e->fft_stream));
+        CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_fft, 0));  // lags below read this piece
         const long long n0 = e->submitted;
         e->submitted += piece;
         if (compat) {
@@ -722,6 +748,7 @@ extern "C" int ddm_reset_accumulators(ddm_engine *e) {
 extern "C" int ddm_synchronize(ddm_engine *e) {
     clear_error();
     if (!e) return fail(DDM_ERR_INVALID_ARG, "null engine");
+    CUDA_TRY(cudaStreamSynchronize(e->fft_stream));
     CUDA_TRY(cudaStreamSynchronize(e->stream));
     CUDA_TRY(cudaGetLastError());
     return check_device_status(e);
@@ -758,6 +785,7 @@ extern "C" int ddm_read_spectrum(ddm_engine *e, int frame, float *out, long capa
     if (!e || !out || capacity < 2 * e->E) return fail(DDM_ERR_INVALID_ARG, "bad argument");
     if (frame < 0 || frame >= e->submitted || frame < e->submitted - e->R)
         return fail(DDM_ERR_INVALID_ARG, "frame is not in the ring");
+    CUDA_TRY(cudaStreamSynchronize(e->fft_stream));
     CUDA_TRY(cudaStreamSynchronize(e->stream));
     CUDA_TRY(cudaMemcpy(out, e->ring + static_cast<size_t>(frame % e->R) * e->E, sizeof(float2) * e->E,
                         cudaMemcpyDeviceToHost));

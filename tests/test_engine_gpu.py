@@ -106,7 +106,7 @@ def test_unbiased_multiscale_matches_oracle():
     isf, _, info = engine_run(frames, scales, taus, lambdas, estimator="unbiased", C=10)
     want, _ = O.ddm_run(frames, scales, taus, lambdas, estimator=O.EST_UNBIASED, chunk=10)
     assert_isf_close(isf, want, scales, len(lambdas), len(taus))
-    assert info.ring_slots == 55 + 10
+    assert info.ring_slots == 55 + 2 * 10  # tau_max + one piece + one piece of FFT overlap
 
 
 def test_u16_full_precision_matches_oracle():
