@@ -206,6 +206,10 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
     rows.pixmode = e->pixmode;
     rows.x_off = x_off;
     rows.y_off = y_off;
+    rows.vec4 = (e->bpp == 1 && x_off % 4 == 0 && row_pitch % 4 == 0 && frame_stride % 4 == 0 &&
+                 reinterpret_cast<uintptr_t>(src) % 4 == 0)
+                    ? 1
+                    : 0;
     rows.ring = e->ring;
     rows.E = e->E;
     rows.R = e->R;

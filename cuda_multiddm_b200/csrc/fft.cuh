@@ -198,6 +198,7 @@ struct FftArgs {
     const uint8_t *src;
     long long frame_stride, row_pitch;
     int bpp, pixmode, x_off, y_off;
+    int vec4;  // 1: bpp == 1 and every row start is 4-byte aligned (vectorised pixel loads)
     // ring
     float2 *ring;
     long long E;
@@ -227,7 +228,34 @@ __device__ __forceinline__ void fft_rows_body(const FftArgs &a, const FftScale &
     const int total_pairs = (1 << (2 * sc.log2side)) * (L / 2);
     const int g0 = (blockIdx.x - sc.cta_begin) * NT;
     const uint8_t *fsrc = a.src + blockIdx.y * a.frame_stride;
-#pragma unroll 4
+    if constexpr (L >= 4) {
+        if (a.vec4) {  // one byte per pixel, 4-byte aligned rows: 4 pixels of each row per load
+#pragma unroll
+            for (int it = 0; it < ITER / 4; it++) {
+                const int q = threadIdx.x + it * kFftThreads;
+                const int c = q >> (LOG2L - 2), i = (q & (L / 4 - 1)) * 4;
+                const int g = g0 + c;
+                uchar4 r0 = make_uchar4(0, 0, 0, 0), r1 = r0;
+                if (g < total_pairs) {
+                    const int tile = g >> (LOG2L - 1);
+                    const int py = 2 * (g & (L / 2 - 1));
+                    const int ty = tile >> sc.log2side, tx = tile & (sc.tiles_side - 1);
+                    const long long Y = (static_cast<long long>(ty) << LOG2L) + py + a.y_off;
+                    const long long X = (static_cast<long long>(tx) << LOG2L) + i + a.x_off;
+                    const uint8_t *p0 = fsrc + Y * a.row_pitch + X;
+                    r0 = *reinterpret_cast<const uchar4 *>(p0);
+                    r1 = *reinterpret_cast<const uchar4 *>(p0 + a.row_pitch);
+                }
+                float2 *d = fsm + c * TS + fpad(i);  // i .. i+3 share one 16-element pad block
+                d[0] = make_float2(r0.x, r1.x);
+                d[1] = make_float2(r0.y, r1.y);
+                d[2] = make_float2(r0.z, r1.z);
+                d[3] = make_float2(r0.w, r1.w);
+            }
+            goto loaded;
+        }
+    }
+#pragma unroll
     for (int it = 0; it < ITER; it++) {
         const int q = threadIdx.x + it * kFftThreads;
         const int c = q >> LOG2L, i = q & (L - 1);
@@ -244,6 +272,7 @@ __device__ __forceinline__ void fft_rows_body(const FftArgs &a, const FftScale &
         }
         fsm[c * TS + fpad(i)] = z;
     }
+loaded:
     __syncthreads();
     const int c_me = threadIdx.x / TEAM, t = threadIdx.x & (TEAM - 1);
     float2 *buf = fsm + c_me * TS;
@@ -278,7 +307,7 @@ __device__ __forceinline__ void fft_cols_body(const FftArgs &a, const FftScale &
     const int g0 = (blockIdx.x - sc.cta_begin) * NT;
     const long long slot = (a.first_label + blockIdx.y) % a.R;
     float2 *base = a.ring + slot * a.E + sc.off;
-#pragma unroll 4
+#pragma unroll
     for (int it = 0; it < ITER; it++) {
         const int q = threadIdx.x + it * kFftThreads;
         const int y = q >> LOG2NT, c = q & (NT - 1);
@@ -293,7 +322,7 @@ __device__ __forceinline__ void fft_cols_body(const FftArgs &a, const FftScale &
     __syncthreads();
     const int c_me = threadIdx.x / TEAM, t = threadIdx.x & (TEAM - 1);
     fft_transform<LOG2L>(fsm + c_me * TS, t, a.tw + (L - 2));
-#pragma unroll 4
+#pragma unroll
     for (int it = 0; it < ITER; it++) {
         const int q = threadIdx.x + it * kFftThreads;
         const int y = q >> LOG2NT, c = q & (NT - 1);

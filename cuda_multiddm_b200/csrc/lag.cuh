@@ -259,13 +259,14 @@ __global__ void __launch_bounds__(kLagThreads, 3)
             if (!ok) *abort_flag = 1;
             if (*abort_flag) break;
             const uint32_t o = static_cast<uint32_t>(ub) * kLagSlotBytes;
-            unsigned long long acc2 = 0ull;
+            // four independent packed accumulators (j mod 4) keep the FMA pipeline full
+            unsigned long long acc2[4] = {0ull, 0ull, 0ull, 0ull};
             if (ent_full[e]) {  // nreg == J, every register frame and partner present
 #pragma unroll
                 for (int j = 0; j < J; j++) {
                     const uint32_t off = ((o + j * kLagSlotBytes) & kLagRingMask) | toff;
                     const unsigned long long b = *reinterpret_cast<const unsigned long long *>(smem + off);
-                    acc2 = f2_fma_sq(f2_sub(r[j], b), acc2);
+                    acc2[j & 3] = f2_fma_sq(f2_sub(r[j], b), acc2[j & 3]);
                 }
             } else {
 #pragma unroll
@@ -273,11 +274,11 @@ __global__ void __launch_bounds__(kLagThreads, 3)
                     if (j < nreg && tab[kTabReg + j] >= 0 && uslot[ub + j] >= 0) {
                         const uint32_t off = ((o + j * kLagSlotBytes) & kLagRingMask) | toff;
                         const unsigned long long b = *reinterpret_cast<const unsigned long long *>(smem + off);
-                        acc2 = f2_fma_sq(f2_sub(r[j], b), acc2);
+                        acc2[j & 3] = f2_fma_sq(f2_sub(r[j], b), acc2[j & 3]);
                     }
                 }
             }
-            const float sum = f2_hsum(acc2);
+            const float sum = (f2_hsum(acc2[0]) + f2_hsum(acc2[1])) + (f2_hsum(acc2[2]) + f2_hsum(acc2[3]));
             // Kahan step: a.x running sum, a.y compensation (true value a.x - a.y)
             const float y = sum - a0.y;
             const float t = a0.x + y;
