@@ -233,9 +233,11 @@ int main(int argc, char **argv) {
         buf[i] = static_cast<uint8_t *>(ddm_host_alloc(frame_bytes * chunk));
         if (!buf[i]) die(ddm_last_error());
     }
-    if (bench) {  // src/DDM.cu:522-528 fills the first frame with rand() % 255
-        for (int i = 0; i < 2; i++)
-            for (size_t k = 0; k < frame_bytes * chunk; k++) buf[i][k] = static_cast<uint8_t>(std::rand() % 255);
+    if (bench) {  // as src/DDM.cu:522-528: the first frame of each buffer gets rand() % 255
+        for (int i = 0; i < 2; i++) {
+            std::memset(buf[i], 0, frame_bytes * chunk);
+            for (size_t k = 0; k < frame_bytes; k++) buf[i][k] = static_cast<uint8_t>(std::rand() % 255);
+        }
     }
     const float int_fps = static_cast<float>(static_cast<int>(fps));  // analyse_accums takes int (src/DDM.cu:79)
     std::vector<double> isf(ddm_isf_size(eng));
