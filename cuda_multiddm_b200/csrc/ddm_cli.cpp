@@ -271,8 +271,9 @@ int main(int argc, char **argv) {
         if (ddm_submit_frames(eng, buf[which], n, 0) != DDM_OK) die(ddm_last_error());
         sent += n;
         which ^= 1;
-        // the other buffer is refilled next: its copy must have finished
-        if (ddm_synchronize(eng) != DDM_OK) die(ddm_last_error());
+        // the other buffer is refilled next: its copy must have finished (benchmark mode
+        // never refills its buffers)
+        if (!bench && ddm_synchronize(eng) != DDM_OK) die(ddm_last_error());
         while (dumps_written < ddm_dump_count(eng)) {  // -G snapshots, src/DDM.cu:800-826
             if (ddm_read_dump(eng, dumps_written, isf.data(), static_cast<long>(isf.size())) != DDM_OK)
                 die(ddm_last_error());
