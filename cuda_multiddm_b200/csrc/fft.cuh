@@ -40,7 +40,18 @@ __host__ __device__ constexpr int fft_team(int L) { return L >= 16 ? L / 16 : 1;
 __host__ __device__ constexpr int fft_per_cta(int L) {
     return kFftThreads / fft_team(L) < 1 ? 1 : kFftThreads / fft_team(L);
 }
-__host__ __device__ constexpr int kFftPad(int L) { return L + L / 16 + 1; }
+// Distance (in float2) between the transforms of a CTA: at least L + L/16 (padded length),
+// rounded up so that the column pass's transposed accesses -- NT transforms x 16/NT rows per
+// half-warp for NT < 16, 16 transforms for NT >= 16 -- hit 16 distinct 8-byte bank pairs:
+// stride = 16/NT (mod 16) when NT < 16, odd otherwise.
+__host__ __device__ constexpr int kFftPadTarget(int L) {
+    return fft_per_cta(L) < 16 ? 16 / fft_per_cta(L) : 1;
+}
+__host__ __device__ constexpr int kFftPad(int L) {
+    return (L + L / 16 + 1) + ((kFftPadTarget(L) < 16 && fft_per_cta(L) < 16)
+                                   ? ((kFftPadTarget(L) - (L + L / 16 + 1) % 16) + 16) % 16
+                                   : ((L + L / 16 + 1) % 2 == 0 ? 1 : 0));
+}
 __device__ __forceinline__ int fpad(int i) { return i + (i >> 4); }
 
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
@@ -247,10 +258,16 @@ __device__ __forceinline__ void fft_rows_body(const FftArgs &a, const FftScale &
                     r1 = *reinterpret_cast<const uchar4 *>(p0 + a.row_pitch);
                 }
                 float2 *d = fsm + c * TS + fpad(i);  // i .. i+3 share one 16-element pad block
-                d[0] = make_float2(r0.x, r1.x);
-                d[1] = make_float2(r0.y, r1.y);
-                d[2] = make_float2(r0.z, r1.z);
-                d[3] = make_float2(r0.w, r1.w);
+                // thread t = 4a + b stores value (k + a) mod 4 at step k: the 16 threads of a
+                // half-warp then hit 16 distinct bank pairs (a plain d[0..3] order is 4-way)
+                const float2 v[4] = {make_float2(r0.x, r1.x), make_float2(r0.y, r1.y), make_float2(r0.z, r1.z),
+                                     make_float2(r0.w, r1.w)};
+                const int a4 = (threadIdx.x >> 2) & 3;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const int m = (k + a4) & 3;
+                    d[m] = m == 0 ? v[0] : m == 1 ? v[1] : m == 2 ? v[2] : v[3];
+                }
             }
             goto loaded;
         }
@@ -351,13 +368,13 @@ __device__ __forceinline__ void fft_cols_body(const FftArgs &a, const FftScale &
     }
 
 // grid (sum of ctas_per_frame, frames)
-__global__ void __launch_bounds__(kFftThreads) fft_rows_kernel(FftArgs a) {
+__global__ void __launch_bounds__(kFftThreads, 3) fft_rows_kernel(FftArgs a) {
     extern __shared__ float2 fsm[];
     const FftScale &sc = a.sc[fft_find_scale(a)];
     DDM_FFT_DISPATCH(fft_rows_body)
 }
 
-__global__ void __launch_bounds__(kFftThreads) fft_cols_kernel(FftArgs a) {
+__global__ void __launch_bounds__(kFftThreads, 3) fft_cols_kernel(FftArgs a) {
     extern __shared__ float2 fsm[];
     const FftScale &sc = a.sc[fft_find_scale(a)];
     DDM_FFT_DISPATCH(fft_cols_body)

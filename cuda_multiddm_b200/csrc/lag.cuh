@@ -261,7 +261,16 @@ __global__ void __launch_bounds__(kLagThreads, 3)
             const uint32_t o = static_cast<uint32_t>(ub) * kLagSlotBytes;
             // four independent packed accumulators (j mod 4) keep the FMA pipeline full
             unsigned long long acc2[4] = {0ull, 0ull, 0ull, 0ull};
-            if (ent_full[e]) {  // nreg == J, every register frame and partner present
+            const int s0 = ub & (kLagSlots - 1);
+            if (ent_full[e] && s0 + J <= kLagSlots) {
+                // whole window present and contiguous in the ring: fixed offsets from one base
+                const unsigned char *w = smem + s0 * kLagSlotBytes + toff;
+#pragma unroll
+                for (int j = 0; j < J; j++) {
+                    const unsigned long long b = *reinterpret_cast<const unsigned long long *>(w + j * kLagSlotBytes);
+                    acc2[j & 3] = f2_fma_sq(f2_sub(r[j], b), acc2[j & 3]);
+                }
+            } else if (ent_full[e]) {  // nreg == J, every register frame and partner present
 #pragma unroll
                 for (int j = 0; j < J; j++) {
                     const uint32_t off = ((o + j * kLagSlotBytes) & kLagRingMask) | toff;

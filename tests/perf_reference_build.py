@@ -36,7 +36,7 @@ OURS = ROOT / "cuda_multiddm_b200" / "ddm"
 CONFIGS = [
     # name, scales, taus, lambdas, (N small, N large), C (the reference needs C >= tau_max)
     ("single_256_tau20", [256], list(range(1, 21)), log_lambdas(4, 128, 10), (2000, 20000), 20),
-    ("single_1024_tau64_log500", [1024], log_taus(1, 500, 64), log_lambdas(2, 512, 30), (2000, 6000), 500),
+    ("single_1024_tau64_log500", [1024], log_taus(1, 500, 64), log_lambdas(2, 512, 30), (2000, 20000), 500),
 ]
 
 
