@@ -258,11 +258,12 @@ __device__ __forceinline__ void fft_rows_body(const FftArgs &a, const FftScale &
                     r1 = *reinterpret_cast<const uchar4 *>(p0 + a.row_pitch);
                 }
                 float2 *d = fsm + c * TS + fpad(i);  // i .. i+3 share one 16-element pad block
-                // thread t = 4a + b stores value (k + a) mod 4 at step k: the 16 threads of a
-                // half-warp then hit 16 distinct bank pairs (a plain d[0..3] order is 4-way)
+                // In order d[0..3], the one-float2 pad per 16 elements already spreads a
+                // half-warp's stores over 16 bank pairs -- except at L = 32, where two
+                // transforms share a half-warp; there thread t = 4a + b stores value (k + a) mod 4.
                 const float2 v[4] = {make_float2(r0.x, r1.x), make_float2(r0.y, r1.y), make_float2(r0.z, r1.z),
                                      make_float2(r0.w, r1.w)};
-                const int a4 = (threadIdx.x >> 2) & 3;
+                const int a4 = L == 32 ? (threadIdx.x >> 2) & 3 : 0;
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
                     const int m = (k + a4) & 3;
