@@ -93,7 +93,11 @@ struct ddm_engine {
     cudaEvent_t tab_ev[kTables] = {};
     bool tab_used[kTables] = {};
     int tab_stride = 0, tab_next = 0;
-    int *q_ptr_d = nullptr, *idx_d = nullptr, *counts_d = nullptr;
+    int *idx_d = nullptr, *counts_d = nullptr;                  // annulus CSR indices, pixel counts
+    int *chunk_beg_d = nullptr, *chunk_end_d = nullptr;          // azimuthal chunks of the CSR
+    int *chunk_first_d = nullptr, *chunk_count_d = nullptr;      // per (scale, q)
+    double *partial_d = nullptr;                                 // stage-1 azimuthal sums
+    long long az_items = 0;
     double *norm_d = nullptr, *isf_d = nullptr;
     int *status_d = nullptr;                // set by kernels whose bounded waits ran out
     LagMaps maps;                           // 2-D tensor maps of the ring for the lag kernel
@@ -145,7 +149,11 @@ void free_all(ddm_engine *e) {
     cudaFree(e->tw);
     cudaFree(e->stage);
     cudaFree(e->tables_d);
-    cudaFree(e->q_ptr_d);
+    cudaFree(e->chunk_beg_d);
+    cudaFree(e->chunk_end_d);
+    cudaFree(e->chunk_first_d);
+    cudaFree(e->chunk_count_d);
+    cudaFree(e->partial_d);
     cudaFree(e->idx_d);
     cudaFree(e->counts_d);
     cudaFree(e->norm_d);
@@ -365,25 +373,30 @@ int run_azimuth(ddm_engine *e, const std::vector<double> &norm) {
     a.S = e->S;
     a.T = e->T;
     a.Q = e->Q;
-    int blocks = 0;
-    for (int s = 0; s < e->S; s++) {
-        a.sc[s] = e->sd[s];
-        a.block_prefix[s] = blocks;
-        blocks += e->sd[s].tiles * e->T;
-    }
-    a.block_prefix[e->S] = blocks;
+    for (int s = 0; s < e->S; s++) a.sc[s] = e->sd[s];
     a.acc = e->acc;
     a.E = e->E;
-    a.q_ptr = e->q_ptr_d;
     a.idx = e->idx_d;
+    a.chunk_beg = e->chunk_beg_d;
+    a.chunk_end = e->chunk_end_d;
+    a.chunk_first = e->chunk_first_d;
+    a.chunk_count = e->chunk_count_d;
     a.counts = e->counts_d;
     a.norm = e->norm_d;
+    a.partial = e->partial_d;
     a.isf = e->isf_d;
+    a.items = e->az_items;
+    a.bins = e->isf_size;
     TimedRange tr(e, 2);
-    azimuth_kernel<<<blocks, kAzThreads, 0, e->stream>>>(a);
+    if (a.items > 0) {
+        azimuth_partial_kernel<<<static_cast<unsigned>((a.items + kAzWarps - 1) / kAzWarps), kAzThreads, 0,
+                                 e->stream>>>(a);
+        CUDA_TRY(cudaGetLastError());
+    }
+    azimuth_final_kernel<<<static_cast<unsigned>((a.bins + kAzThreads - 1) / kAzThreads), kAzThreads, 0, e->stream>>>(a);
     CUDA_TRY(cudaGetLastError());
-    tr.end(1);
-    e->launches++;
+    tr.end(a.items > 0 ? 2 : 1);
+    e->launches += a.items > 0 ? 2 : 1;
     // pageable source: make sure the copy has consumed host_norm before it can change
     CUDA_TRY(cudaStreamSynchronize(e->stream));
     return DDM_OK;
@@ -597,26 +610,49 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
             return bail(fail(DDM_ERR_CUDA, "twiddle upload failed"));
     }
 
-    // Masks (bit-exact host construction) as CSR per (scale, q)
+    // Masks (bit-exact host construction) as CSR per (scale, q), cut into chunks of at most
+    // kAzChunk indices for the two-stage azimuthal reduction
     {
-        std::vector<int> q_ptr_all, idx_all;
+        std::vector<int> idx_all, cbeg, cend, cfirst, ccount;
+        long long items = 0;
         for (int s = 0; s < e->S; s++) {
             std::vector<int> qp, idx, counts;
             build_masks(e->scales[s], e->lambdas, e->tol, &qp, &idx, &counts);
             const int base = static_cast<int>(idx_all.size());
-            for (int q = 0; q <= e->Q; q++) q_ptr_all.push_back(base + qp[q]);
+            ScaleDesc &d = e->sd[s];
+            d.chunk_off = static_cast<int>(cbeg.size());
+            int nloc = 0;
+            for (int q = 0; q < e->Q; q++) {
+                cfirst.push_back(nloc);
+                int n = 0;
+                for (int b = qp[q]; b < qp[q + 1]; b += kAzChunk, n++) {
+                    cbeg.push_back(base + b);
+                    cend.push_back(base + std::min(b + kAzChunk, qp[q + 1]));
+                }
+                ccount.push_back(n);
+                nloc += n;
+            }
+            d.nchunks = nloc;
+            d.item_base = items;
+            items += static_cast<long long>(d.tiles) * e->T * nloc;
             idx_all.insert(idx_all.end(), idx.begin(), idx.end());
             e->counts_h.insert(e->counts_h.end(), counts.begin(), counts.end());
             e->q_ptr_s.push_back(qp);
             e->idx_s.push_back(std::move(idx));
         }
-        if ((st = dev_alloc(e, &e->q_ptr_d, q_ptr_all.size()))) return bail(st);
-        if ((st = dev_alloc(e, &e->idx_d, idx_all.size()))) return bail(st);
-        if ((st = dev_alloc(e, &e->counts_d, e->counts_h.size()))) return bail(st);
-        if (cudaMemcpy(e->q_ptr_d, q_ptr_all.data(), sizeof(int) * q_ptr_all.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-            (!idx_all.empty() && cudaMemcpy(e->idx_d, idx_all.data(), sizeof(int) * idx_all.size(), cudaMemcpyHostToDevice) != cudaSuccess) ||
-            cudaMemcpy(e->counts_d, e->counts_h.data(), sizeof(int) * e->counts_h.size(), cudaMemcpyHostToDevice) != cudaSuccess)
-            return bail(fail(DDM_ERR_CUDA, "mask upload failed"));
+        e->az_items = items;
+        auto up = [&](int **dst, const std::vector<int> &v) {
+            int r = dev_alloc(e, dst, v.size());
+            if (r) return r;
+            if (!v.empty() && cudaMemcpy(*dst, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+                return fail(DDM_ERR_CUDA, "mask upload failed");
+            return static_cast<int>(DDM_OK);
+        };
+        if ((st = up(&e->idx_d, idx_all)) || (st = up(&e->chunk_beg_d, cbeg)) || (st = up(&e->chunk_end_d, cend)) ||
+            (st = up(&e->chunk_first_d, cfirst)) || (st = up(&e->chunk_count_d, ccount)) ||
+            (st = up(&e->counts_d, e->counts_h)))
+            return bail(st);
+        if ((st = dev_alloc(e, &e->partial_d, static_cast<size_t>(std::max<long long>(items, 1))))) return bail(st);
     }
 
     // Kernel shared-memory limits (the FFT passes use up to 128 KB)

@@ -178,6 +178,6 @@ def test_kernel_launches_counted():
     frames = media.synth_video(2, 64, 64, 8, 10)
     _, _, info = engine_run(frames, [64, 32], [1, 2], [4.0], estimator="unbiased", C=4)
     # per piece of 4 frames: one row-pass and one column-pass launch over all scales (the
-    # 4 frames fit one L2-resident group) + 1 lag launch; then 1 azimuthal launch
-    assert info.kernel_launches == 2 * (2 + 1) + 1
+    # 4 frames fit one L2-resident group) + 1 lag launch; then the two azimuthal stages
+    assert info.kernel_launches == 2 * (2 + 1) + 2
     assert lib() is not None
