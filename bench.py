@@ -156,6 +156,19 @@ def cpu_baseline(seconds_hint: float = 20.0) -> dict:
                       f"(extract + R2C FFT at every scale + 64 lag pairs per frame), OpenMP {threads} threads"}
 
 
+def job_throughput(times_ms, frames_per_rank: int, world: int, device=None):
+    """Whole-job throughput of `world` ranks that each analysed frames_per_rank frames:
+    every timing is reduced to its maximum over ranks (the job ends when the slowest rank
+    does). Returns (value, e2e_value, max_ms, max_e2e_ms) for times_ms = [device, e2e]."""
+    import torch
+    t = torch.tensor(times_ms, dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total = frames_per_rank * world
+    return total / (float(t[0]) / 1000.0), total / (float(t[1]) / 1000.0), float(t[0]), float(t[1])
+
+
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -266,13 +279,8 @@ def run_ours(args) -> None:
     e2e_ms = e0.elapsed_time(e1)
 
     # ---- max over ranks ---------------------------------------------------------------
-    t = torch.tensor([elapsed_ms, e2e_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    elapsed_ms, e2e_ms = float(t[0]), float(t[1])
-    frames_total = args.steps * CHUNK * world
-    value = frames_total / (elapsed_ms / 1000.0)
-    e2e_value = frames_total / (e2e_ms / 1000.0)
+    value, e2e_value, elapsed_ms, e2e_ms = job_throughput(
+        [elapsed_ms, e2e_ms], args.steps * CHUNK, world, "cuda" if world > 1 else None)
 
     lag_ms, lag_n = ktimes["lag"]
     lag_avg_s = lag_ms / 1000.0 / max(lag_n, 1)
