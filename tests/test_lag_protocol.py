@@ -1,0 +1,317 @@
+"""CPU checks of the lag kernel's launch tables and its shared-memory pipeline protocol.
+
+The lag kernel (cuda_multiddm_b200/csrc/lag.cuh) streams the distinct partner frames of a
+launch (the "union") through 8 groups of 8 shared-memory slots: one producer lane issues
+each group's 2-D TMA boxes and arms the group's *full* barrier; four consumer warps wait on
+every group their window reaches and arrive on the group's *empty* barrier once no later
+window reads it. These tests build the tables with the engine's own C++ builder
+(``build_lag_table``, csrc/lag_host.hpp, driven by tests/lag_table_probe.cu) for the
+schedules the engine launches — causal windows (unbiased estimator) and the reference's
+start|end windows (src/DDM.cu:250-255) — plus random windows with holes, and check
+
+* every window maps union entries back to the ring slots of its positions,
+* the TMA runs cover exactly the union entries that hold a frame, inside their group,
+* the "full window" flag is right (it selects the kernel's unchecked fast paths),
+* the table fits the kernel's shared-memory limit,
+* a replay of the barrier protocol (mbarrier phase parity as the hardware defines it) under
+  random interleavings of the producer and the four consumer warps neither deadlocks nor
+  lets a consumer read a slot that holds another group's data.
+"""
+from __future__ import annotations
+
+import random
+import subprocess
+from pathlib import Path
+
+import pytest
+
+from cuda_multiddm_b200.media import log_taus
+
+ROOT = Path(__file__).resolve().parents[1]
+CSRC = ROOT / "cuda_multiddm_b200" / "csrc"
+PROBE_SRC = ROOT / "tests" / "lag_table_probe.cu"
+PROBE = ROOT / "tests" / "_build" / "lag_table_probe"
+
+# constants of csrc/lag.cuh
+SLOTS, GROUP, GROUP_SLOTS, CONSUMERS = 64, 8, 8, 4
+LAG_JS = (4, 8, 16, 20, 24, 30, 32)
+SLOT_BYTES, SMEM_MAX = 1024, 220 * 1024
+TAB_ENTRIES = 5 + 32
+
+
+def pick_j(nreg: int) -> int:
+    return next(j for j in LAG_JS if j >= nreg)
+
+
+@pytest.fixture(scope="module")
+def probe() -> Path:
+    deps = [PROBE_SRC, CSRC / "lag_host.hpp", CSRC / "lag.cuh"]
+    if not PROBE.exists() or PROBE.stat().st_mtime < max(p.stat().st_mtime for p in deps):
+        PROBE.parent.mkdir(parents=True, exist_ok=True)
+        subprocess.run(["nvcc", "-std=c++17", "-O1", "-gencode", "arch=compute_100a,code=sm_100a",
+                        "-I", str(CSRC), str(PROBE_SRC), "-o", str(PROBE)], check=True)
+    return PROBE
+
+
+def build_tables(probe: Path, cases: list[dict]) -> list[list[int] | str]:
+    lines = []
+    for c in cases:
+        nreg = c["nreg"]
+        vals = [nreg, pick_j(nreg), len(c["ent_acc"]), len(c["pos"])]
+        vals += c["reg"][:nreg] + c["ent_acc"] + c["ent_w"] + c["pos"]
+        lines.append(" ".join(map(str, vals)))
+    out = subprocess.run([str(probe)], input="\n".join(lines) + "\n", capture_output=True, text=True,
+                         check=True).stdout.splitlines()
+    assert len(out) == len(cases)
+    return [o if o.startswith("ERR") else [int(v) for v in o.split()] for o in out]
+
+
+def parse(t: list[int]) -> dict:
+    nreg, ntau, nu, ngroups, nruns = t[:5]
+    p = TAB_ENTRIES
+    d = {"nreg": nreg, "ntau": ntau, "nu": nu, "ngroups": ngroups, "reg": t[5:5 + 32]}
+    for name, n in (("ent_acc", ntau), ("ub", ntau), ("full", ntau), ("uslot", nu),
+                    ("gptr", ngroups + 1), ("runs", nruns)):
+        d[name] = t[p:p + n]
+        p += n
+    assert p == len(t)
+    return d
+
+
+# ---------------------------------------------------------------------------------------
+# launch descriptions, as csrc/engine.cu builds them
+# ---------------------------------------------------------------------------------------
+
+def causal_case(taus: list[int], n0: int, c: int, R: int) -> dict:
+    """lag_causal: frames n0..n0+c-1 against every tau, windows in descending tau."""
+    tmax, T = max(taus), len(taus)
+    slot = lambda f: f % R if f >= 0 else -1  # noqa: E731
+    return {"nreg": c, "reg": [slot(n0 + j) for j in range(c)],
+            "ent_acc": list(range(T - 1, -1, -1)),
+            "ent_w": [tmax - taus[i] for i in range(T - 1, -1, -1)],
+            "pos": [slot(n0 - tmax + p) for p in range(c + tmax)]}
+
+
+def compat_case(taus: list[int], start: list[int], end: list[int], f0: int, R: int) -> dict:
+    """lag_iteration: A = start[f0..], partner of position q = start|end[q]."""
+    C = len(start)
+    nreg = min(32, C - f0)
+    slot = lambda f: f % R if f >= 0 else -1  # noqa: E731
+    pos = []
+    for p in range(nreg + max(taus)):
+        q = f0 + p
+        lab = start[q] if q < C else (end[q - C] if q - C < C else -1)
+        pos.append(slot(lab))
+    return {"nreg": nreg, "reg": [slot(start[f0 + j]) for j in range(nreg)],
+            "ent_acc": list(range(len(taus))), "ent_w": list(taus), "pos": pos}
+
+
+def random_case(rnd: random.Random) -> dict:
+    nreg = rnd.choice([1, 3, 4, 7, 8, 16, 20, 29, 30, 32])
+    ntau = rnd.randint(1, 70)
+    starts = sorted(rnd.sample(range(0, 600), ntau))
+    npos = starts[-1] + nreg
+    R = rnd.choice([40, 97, 530, 4096])
+    base = rnd.randrange(R)
+    hole = rnd.random() * 0.3
+    pos = [-1 if rnd.random() < hole else (base + p) % R for p in range(npos)]
+    reg = [-1 if rnd.random() < hole / 3 else rnd.randrange(R) for _ in range(nreg)]
+    return {"nreg": nreg, "reg": reg, "ent_acc": [rnd.randrange(128) for _ in range(ntau)],
+            "ent_w": starts, "pos": pos}
+
+
+def schedule_cases() -> list[dict]:
+    cases = []
+    tau_sets = [log_taus(1, 500, 64), [1, 2, 3, 5, 8, 13, 21, 34, 55], list(range(1, 21)),
+                log_taus(1, 300, 48), [1], [7, 300]]
+    for taus in tau_sets:
+        for c in (30, 32, 20, 8, 1, 3):
+            R = max(taus) + 2 * c
+            for n0 in (0, 7, 30, 200, 600, 1000):
+                cases.append(causal_case(taus, n0, c, R))
+    for taus, C in ((list(range(1, 21)), 20), ([1, 2, 4, 8, 16, 32], 40), ([1, 3, 9], 10), ([2, 5], 64)):
+        R = 3 * C + 5
+        for base in (0, 7 * C):
+            start = [base + i for i in range(C)]
+            for end in ([base + C + i for i in range(C)], [-1] * C,            # tail: nothing yet
+                        [base + 2 * C + i for i in range(C)]):                 # stale pinned buffer
+                for f0 in range(0, C, 32):
+                    cases.append(compat_case(taus, start, end, f0, R))
+    rnd = random.Random(1234)
+    cases += [random_case(rnd) for _ in range(150)]
+    return cases
+
+
+# ---------------------------------------------------------------------------------------
+# checks
+# ---------------------------------------------------------------------------------------
+
+def check_table(case: dict, d: dict) -> None:
+    nreg, J = case["nreg"], pick_j(case["nreg"])
+    assert d["nreg"] == nreg and d["ntau"] == len(case["ent_acc"])
+    assert d["reg"][:nreg] == case["reg"][:nreg] and all(v == -1 for v in d["reg"][nreg:])
+    assert d["ent_acc"] == case["ent_acc"]
+    nu, ub, us = d["nu"], d["ub"], d["uslot"]
+    for e, w in enumerate(case["ent_w"]):
+        assert 0 <= ub[e] and ub[e] + nreg <= nu
+        if e:
+            assert ub[e] > ub[e - 1]
+        assert us[ub[e]:ub[e] + nreg] == case["pos"][w:w + nreg]
+        full = nreg == J and all(r >= 0 for r in case["reg"][:nreg]) and all(s >= 0 for s in us[ub[e]:ub[e] + nreg])
+        assert d["full"][e] == int(full)
+    # the union holds each window position once: its size is the number of distinct positions
+    covered = set()
+    for w in case["ent_w"]:
+        covered.update(range(w, w + nreg))
+    assert nu == len(covered)
+    assert d["ngroups"] == (nu + GROUP - 1) // GROUP
+    seen = set()
+    for g in range(d["ngroups"]):
+        for run in d["runs"][d["gptr"][g]:d["gptr"][g + 1]]:
+            slot, rows, rel = run & 0xFFFFF, 1 << ((run >> 20) & 3), (run >> 22) & 7
+            assert rel + rows <= GROUP
+            for i in range(rows):
+                u = g * GROUP + rel + i
+                assert u < nu and us[u] == slot + i and u not in seen
+                seen.add(u)
+    assert seen == {u for u in range(nu) if us[u] >= 0}
+    ntab = TAB_ENTRIES + 3 * d["ntau"] + nu + d["ngroups"] + 1 + len(d["runs"])
+    assert 1024 + SLOTS * SLOT_BYTES + 2 * 8 * GROUP_SLOTS + 4 * (1 + ntab) <= SMEM_MAX
+
+
+def parity_done(completed: int, parity: int) -> bool:
+    """mbarrier try_wait.parity P returns once the phase with parity P has completed."""
+    return completed >= 1 and (completed - 1) % 2 == parity
+
+
+def replay(d: dict, seed: int) -> str:
+    """Random interleaving of the producer lane and the consumer warps, as lag_pipe_kernel."""
+    rnd = random.Random(seed)
+    nreg, ntau, nu, ngroups, ub = d["nreg"], d["ntau"], d["nu"], d["ngroups"], d["ub"]
+    full_c, empty_c, empty_arr = [0] * GROUP_SLOTS, [0] * GROUP_SLOTS, [0] * GROUP_SLOTS
+    content = [None] * GROUP_SLOTS  # which group a group slot holds
+    g_next = 0
+    warps = [{"e": 0, "waited": 0, "released": 0} for _ in range(CONSUMERS)]
+    idle = 0
+    while True:
+        actors = (["P"] if g_next < ngroups else []) + [w for w in range(CONSUMERS) if warps[w]["e"] < ntau]
+        if not actors:
+            return "ok"
+        a = rnd.choice(actors)
+        progressed = False
+        if a == "P":
+            gs, fill = g_next % GROUP_SLOTS, g_next // GROUP_SLOTS
+            if fill == 0 or parity_done(empty_c[gs], (fill - 1) & 1):
+                full_c[gs] += 1  # data landed (or bare arrive for a group without frames)
+                content[gs] = g_next
+                g_next += 1
+                progressed = True
+        else:
+            s = warps[a]
+            e = s["e"]
+            glast = (ub[e] + nreg - 1) // GROUP
+            if all(parity_done(full_c[g % GROUP_SLOTS], (g // GROUP_SLOTS) & 1) for g in range(s["waited"], glast + 1)):
+                s["waited"] = max(s["waited"], glast + 1)
+                for j in range(nreg):
+                    u = ub[e] + j
+                    if d["uslot"][u] >= 0 and content[(u // GROUP) % GROUP_SLOTS] != u // GROUP:
+                        return f"stale read of union entry {u} by entry {e}"
+                next_g = (ub[e + 1] if e + 1 < ntau else nu) // GROUP
+                for g in range(s["released"], next_g):
+                    gs = g % GROUP_SLOTS
+                    empty_arr[gs] += 1
+                    if empty_arr[gs] == CONSUMERS:
+                        empty_arr[gs] = 0
+                        empty_c[gs] += 1
+                s["released"] = max(s["released"], next_g)
+                s["e"] += 1
+                progressed = True
+        idle = 0 if progressed else idle + 1
+        if idle > 4000:
+            return "deadlock"
+
+
+def test_tables_and_protocol(probe):
+    cases = schedule_cases()
+    tables = build_tables(probe, cases)
+    for i, (case, t) in enumerate(zip(cases, tables)):
+        assert not isinstance(t, str), (i, t)
+        d = parse(t)
+        check_table(case, d)
+        for seed in range(2):
+            assert replay(d, seed) == "ok", (i, seed)
+
+
+def test_windows_must_ascend(probe):
+    case = causal_case([1, 2, 3], 10, 4, 20)
+    case["ent_w"] = case["ent_w"][::-1]
+    assert build_tables(probe, [case])[0] == "ERR lag windows out of order"
+
+
+def test_union_shrinks_reads():
+    """The union is what makes the kernel read fewer bytes than one frame per pair: a
+    30-frame chunk against 64 log-spaced taus up to 500 needs 484 partner frames, not 1920."""
+    taus = log_taus(1, 500, 64)
+    case = causal_case(taus, 1000, 30, 560)
+    covered = set()
+    for w in case["ent_w"]:
+        covered.update(range(w, w + 30))
+    assert len(covered) == 484
+
+
+def test_wrong_protocol_is_caught(probe):
+    """The replay catches a consumer that skips waiting on groups without frames (the
+    protocol error the kernel avoids): with it the consumer may release a group slot before
+    the producer has filled it, which shows up as a stale read or a deadlock."""
+    d = parse(build_tables(probe, [causal_case(log_taus(1, 500, 64), 0, 30, 560)])[0])
+    bad = dict(d)
+    # plant the mistake in the model: groups without frames count as already waited on
+    empty_groups = [g for g in range(d["ngroups"]) if d["gptr"][g] == d["gptr"][g + 1]]
+    assert empty_groups, "the case must have groups without frames"
+
+    def replay_skip(seed: int) -> str:
+        rnd = random.Random(seed)
+        nreg, ntau, nu, ngroups, ub = bad["nreg"], bad["ntau"], bad["nu"], bad["ngroups"], bad["ub"]
+        full_c, empty_c, empty_arr = [0] * GROUP_SLOTS, [0] * GROUP_SLOTS, [0] * GROUP_SLOTS
+        content = [None] * GROUP_SLOTS
+        g_next, idle = 0, 0
+        warps = [{"e": 0, "released": 0} for _ in range(CONSUMERS)]
+        while True:
+            actors = (["P"] if g_next < ngroups else []) + [w for w in range(CONSUMERS) if warps[w]["e"] < ntau]
+            if not actors:
+                return "ok"
+            a = rnd.choice(actors)
+            progressed = False
+            if a == "P":
+                gs, fill = g_next % GROUP_SLOTS, g_next // GROUP_SLOTS
+                if fill == 0 or parity_done(empty_c[gs], (fill - 1) & 1):
+                    full_c[gs] += 1
+                    content[gs] = g_next
+                    g_next += 1
+                    progressed = True
+            else:
+                s = warps[a]
+                e = s["e"]
+                glast = (ub[e] + nreg - 1) // GROUP
+                need = [g for g in range(ub[e] // GROUP, glast + 1) if g not in empty_groups]
+                if all(parity_done(full_c[g % GROUP_SLOTS], (g // GROUP_SLOTS) & 1) for g in need):
+                    for j in range(nreg):
+                        u = ub[e] + j
+                        if bad["uslot"][u] >= 0 and content[(u // GROUP) % GROUP_SLOTS] != u // GROUP:
+                            return "stale"
+                    next_g = (ub[e + 1] if e + 1 < ntau else nu) // GROUP
+                    for g in range(s["released"], next_g):
+                        gs = g % GROUP_SLOTS
+                        empty_arr[gs] += 1
+                        if empty_arr[gs] == CONSUMERS:
+                            empty_arr[gs] = 0
+                            empty_c[gs] += 1
+                    s["released"] = max(s["released"], next_g)
+                    s["e"] += 1
+                    progressed = True
+            idle = 0 if progressed else idle + 1
+            if idle > 4000:
+                return "deadlock"
+
+    assert any(replay_skip(seed) != "ok" for seed in range(20))
+    assert all(replay(d, seed) == "ok" for seed in range(20))
