@@ -78,15 +78,16 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per lag launch from the committed ncu summary (None if absent)."""
+def profiled_traffic(frames_per_launch: float):
+    """DRAM bytes per lag launch of `frames_per_launch` frames, from the per-frame DRAM
+    traffic in the committed ncu summary of the lag kernel (None if absent)."""
     p = ROOT / "profiles" / "lag_kernel_c2.txt"
     if not p.exists():
         return None
     for line in p.read_text().splitlines():
-        if line.startswith("traffic_bytes_per_launch:"):
+        if line.startswith("traffic_bytes_per_frame:"):
             try:
-                return float(line.split(":", 1)[1].split()[0])
+                return float(line.split(":", 1)[1].split()[0]) * frames_per_launch
             except ValueError:
                 return None
     return None
@@ -208,7 +209,8 @@ def run_ours(args) -> None:
     dev_video = torch.from_numpy(video).cuda()
     host_video = torch.from_numpy(video).pin_memory()
     cfg = EngineConfig(frame_width=SIDE, frame_height=SIDE, scales=SCALES, taus=taus, lambdas=lambdas,
-                       tolerance=1.2, chunk_frames=CHUNK, estimator="unbiased", device=local)
+                       tolerance=1.2, chunk_frames=CHUNK, estimator="unbiased", device=local,
+                       lag_batch_frames=args.lag_batch)
     eng = Engine(cfg)
     stream = torch.cuda.ExternalStream(eng.info().stream)
     preroll = math.ceil(max(taus) / CHUNK) + 1
@@ -282,9 +284,14 @@ def run_ours(args) -> None:
     value, e2e_value, elapsed_ms, e2e_ms = job_throughput(
         [elapsed_ms, e2e_ms], args.steps * CHUNK, world, "cuda" if world > 1 else None)
 
+    # Lag launches pair up to --lag-batch frames each (with batching, frames wait in the ring
+    # for a full launch and the finalize at the end of the timed region pairs the rest), so
+    # the algorithmic bytes of an average launch are the model's bytes per frame x the
+    # frames per launch.
     lag_ms, lag_n = ktimes["lag"]
     lag_avg_s = lag_ms / 1000.0 / max(lag_n, 1)
-    bytes_per_launch = lag_bytes_per_frame(T) * CHUNK
+    frames_per_launch = args.steps * CHUNK / max(lag_n, 1)
+    bytes_per_launch = lag_bytes_per_frame(T) * frames_per_launch
     hbm_peak, peak_kind = measured_peaks()
     achieved = bytes_per_launch / lag_avg_s / 1e9
 
@@ -295,16 +302,18 @@ def run_ours(args) -> None:
                 "config": {"workload": "multiscale_1024_4scales_64tau" if SIDE == 1024 else
                            "small_512_4scales_64tau (profiling)", "frames": N_FRAMES, "side": SIDE,
                            "scales": SCALES, "taus": T, "tau_max": max(taus), "lambdas": len(lambdas),
-                           "chunk": CHUNK, "estimator": "unbiased", "steady_state": True,
+                           "chunk": CHUNK, "lag_batch_frames": args.lag_batch or min(CHUNK, 32),
+                           "estimator": "unbiased", "steady_state": True,
                            "l2": "inputs larger than L2 (ring of %d frames x %.1f MB)"
                                  % (eng.info().ring_slots, frames_elements() * 8 / 1e6),
                            "parallelism": f"replicas x{world} (independent streams, no collective)"},
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": CHUNK * SIDE * SIDE,
                         "d2h_bytes_per_step": isf_host.nbytes},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                             "frac": achieved / hbm_peak, "traffic": profiled_traffic(),
+                             "frac": achieved / hbm_peak, "traffic": profiled_traffic(frames_per_launch),
                              "kernel": "lag_kernel", "peak_kind": peak_kind,
-                             "bytes_per_launch": bytes_per_launch, "avg_launch_ms": lag_avg_s * 1000.0},
+                             "bytes_per_launch": bytes_per_launch, "frames_per_launch": frames_per_launch,
+                             "avg_launch_ms": lag_avg_s * 1000.0},
                 "kernels_ms": {k: {"total_ms": v[0], "launches": v[1]} for k, v in ktimes.items()},
                 "gpu_launches": int(launches), "clocks": clocks}
         if world == 1 and not args.no_cpu_baseline:
@@ -323,6 +332,9 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--lag-batch", type=int, default=0,
+                    help="frames paired per lag-kernel launch (1..64; 0 = the engine default, one launch "
+                         "per 30-frame piece)")
     ap.add_argument("--workload", choices=["multiscale", "small"], default="multiscale",
                     help="small: 512^2 frames, scales 512..64, same taus and chunk (profiling only)")
     args = ap.parse_args()

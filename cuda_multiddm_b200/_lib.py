@@ -35,6 +35,7 @@ class Config(C.Structure):
         ("tolerance", C.c_float), ("chunk_frames", C.c_int), ("estimator", C.c_int),
         ("multistream", C.c_int), ("total_frames", C.c_int), ("dump_every", C.c_int),
         ("hbm_budget_bytes", C.c_size_t), ("device", C.c_int), ("stream", C.c_void_p),
+        ("lag_batch_frames", C.c_int),
     ]
 
 

@@ -107,6 +107,14 @@ struct ddm_engine {
 
     // stream state
     long long submitted = 0;               // frame labels 0 .. submitted-1 are in (or passed) the ring
+    // Unbiased estimator: frames lag_next .. submitted-1 are in the ring but not paired yet.
+    // Lag launches take up to lag_batch frames (ddm_config.lag_batch_frames; the partner
+    // frames a launch streams are shared by all its register frames). By default it equals
+    // the ingest piece and every piece is paired at once; a larger batch holds frames back
+    // for fuller launches, and flush_lag pairs the rest before any result is read. Compat
+    // iterations are cut into launches of lag_batch A-frames.
+    long long lag_next = 0;
+    int lag_batch = 32;
     long long launches = 0;
     std::vector<double> pair_count;        // unbiased: pairs per tau since the last purge
     std::vector<CompatIteration> its;      // compat schedule
@@ -287,8 +295,8 @@ int launch_lag(ddm_engine *e, const Launch &L) {
     CUDA_TRY(cudaEventRecord(e->tab_ev[ts], e->stream));
     e->tab_used[ts] = true;
 
-    const unsigned blocks = static_cast<unsigned>((e->E + kLagBlock - 1) / kLagBlock);
-    const size_t smem = lag_smem_bytes(ntab);
+    const unsigned blocks = static_cast<unsigned>((e->E + lag_cta_elems(J) - 1) / lag_cta_elems(J));
+    const size_t smem = lag_smem_bytes(J, ntab);
     TimedRange tr(e, 1);
     switch (J) {
 #define LAG_CASE(JJ)                                                                                   \
@@ -296,7 +304,7 @@ int launch_lag(ddm_engine *e, const Launch &L) {
         lag_pipe_kernel<JJ><<<blocks, kLagThreads, smem, e->stream>>>(e->ring, e->acc, e->E, td, e->status_d, \
                                                                        e->maps);                        \
         break;
-        LAG_CASE(4) LAG_CASE(8) LAG_CASE(16) LAG_CASE(20) LAG_CASE(24) LAG_CASE(30) LAG_CASE(32)
+        LAG_CASE(4) LAG_CASE(8) LAG_CASE(16) LAG_CASE(20) LAG_CASE(24) LAG_CASE(30) LAG_CASE(32) LAG_CASE(64)
 #undef LAG_CASE
         default: return fail(DDM_ERR_STATE, "internal: no lag kernel for this frame count");
     }
@@ -340,12 +348,25 @@ int lag_causal(ddm_engine *e, long long n0, int c) {
     return launch_lag(e, L);
 }
 
+// Unbiased: pair every frame still waiting for a lag launch (compat runs the reference's
+// iterations as their frames arrive and holds nothing back).
+int flush_lag(ddm_engine *e) {
+    if (e->estimator != DDM_EST_UNBIASED) return DDM_OK;
+    while (e->lag_next < e->submitted) {
+        const int c = static_cast<int>(std::min<long long>(e->lag_batch, e->submitted - e->lag_next));
+        int st = lag_causal(e, e->lag_next, c);
+        if (st) return st;
+        e->lag_next += c;
+    }
+    return DDM_OK;
+}
+
 // Reference schedule: iteration `it` pairs A = start[fo] with position fo + tau of
 // start|end (src/DDM.cu:250-255).
 int lag_iteration(ddm_engine *e, const CompatIteration &it) {
-    for (int f0 = 0; f0 < it.count; f0 += kMaxJ) {
+    for (int f0 = 0; f0 < it.count; f0 += e->lag_batch) {
         Launch L;
-        L.nreg = std::min(kMaxJ, it.count - f0);
+        L.nreg = std::min(e->lag_batch, it.count - f0);
         for (int j = 0; j < L.nreg; j++) L.reg[j] = slot_of(e, it.start[f0 + j]);
         for (int i = 0; i < e->T; i++) {
             L.ent_acc.push_back(i);
@@ -508,7 +529,7 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
     e->T = static_cast<int>(e->taus.size());
     e->Q = static_cast<int>(e->lambdas.size());
     e->tau_max = e->taus.back();
-    if (lag_smem_bytes(lag_table_capacity(e->T, kMaxJ + e->tau_max)) > static_cast<size_t>(kLagSmemMax))
+    if (lag_smem_bytes(kMaxJ, lag_table_capacity(e->T, kMaxJ + e->tau_max)) > static_cast<size_t>(kLagSmemMax))
         return bail(fail(DDM_ERR_INVALID_ARG, "tau list too long for the lag kernel's shared-memory table"));
 
     // Geometry
@@ -532,7 +553,10 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
     e->isf_size = isf_off;
 
     // Schedule and ring size
-    e->jmax = std::min(kMaxJ, e->C);
+    e->jmax = std::min(kPieceFrames, e->C);
+    if (cfg->lag_batch_frames < 0 || cfg->lag_batch_frames > kMaxJ)
+        return bail(fail(DDM_ERR_INVALID_ARG, "lag_batch_frames must be 0.." + std::to_string(kMaxJ)));
+    e->lag_batch = cfg->lag_batch_frames ? cfg->lag_batch_frames : e->jmax;
     if (compat) {
         e->its = compat_schedule(e->N, e->C, e->multistream, e->G, e->taus, &e->frames_read);
         // Frames arrive in pieces of jmax and iterations run in order, each once every
@@ -546,7 +570,10 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
         }
         e->R = span + e->jmax;  // + one piece: the next piece's FFT overlaps the running lag
     } else {
-        e->R = e->tau_max + 2 * e->jmax;  // window of one piece + one piece of FFT overlap
+        // A lag launch reads its frames and tau_max frames further back while the next
+        // piece's FFT (jmax frames) may already write; with lag_batch > jmax up to
+        // lag_batch - 1 more frames wait in the ring for a fuller launch.
+        e->R = e->tau_max + 2 * e->jmax + (e->lag_batch > e->jmax ? e->lag_batch - 1 : 0);
         e->pair_count.assign(e->T, 0.0);
     }
 
@@ -664,7 +691,8 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
         cudaFuncSetAttribute(lag_pipe_kernel<20>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
         cudaFuncSetAttribute(lag_pipe_kernel<24>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
         cudaFuncSetAttribute(lag_pipe_kernel<30>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
-        cudaFuncSetAttribute(lag_pipe_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess)
+        cudaFuncSetAttribute(lag_pipe_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
+        cudaFuncSetAttribute(lag_pipe_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess)
         return bail(fail(DDM_ERR_CUDA, "cudaFuncSetAttribute failed"));
 
     if (cudaMemsetAsync(e->acc, 0, acc_bytes, e->stream) != cudaSuccess ||
@@ -725,13 +753,17 @@ extern "C" int ddm_submit_frames(ddm_engine *e, const void *frames, int count, i
         if (st) return st;
         CUDA_TRY(cudaEventRecord(e->ev_fft, e->fft_stream));
         CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_fft, 0));  // lags below read this piece
-        const long long n0 = e->submitted;
         e->submitted += piece;
         if (compat) {
             if ((st = run_ready_iterations(e, false))) return st;
         } else {
-            if ((st = lag_causal(e, n0, piece))) return st;
+            while (e->submitted - e->lag_next >= e->lag_batch) {
+                if ((st = lag_causal(e, e->lag_next, e->lag_batch))) return st;
+                e->lag_next += e->lag_batch;
+            }
+            if (e->lag_batch <= e->jmax && (st = flush_lag(e))) return st;  // no batching
             if (e->G > 0 && e->submitted % (static_cast<long long>(e->G) * e->C) == 0) {
+                if ((st = flush_lag(e))) return st;
                 if ((st = snapshot(e, e->pair_count))) return st;
             }
         }
@@ -750,6 +782,7 @@ extern "C" int ddm_finalize(ddm_engine *e) {
         if ((st = run_ready_iterations(e, true))) return st;
         std::fill(norm.begin(), norm.end(), static_cast<double>(e->N));  // src/DDM.cu:875
     } else {
+        if ((st = flush_lag(e))) return st;
         norm = e->pair_count;
     }
     if ((st = run_azimuth(e, norm))) return st;
@@ -782,12 +815,16 @@ extern "C" int ddm_read_dump(ddm_engine *e, int index, double *out, long capacit
 extern "C" int ddm_reset_accumulators(ddm_engine *e) {
     clear_error();
     if (!e) return fail(DDM_ERR_INVALID_ARG, "null engine");
+    int st = flush_lag(e);  // frames submitted before the reset belong to the discarded sums
+    if (st) return st;
     return purge(e);
 }
 
 extern "C" int ddm_synchronize(ddm_engine *e) {
     clear_error();
     if (!e) return fail(DDM_ERR_INVALID_ARG, "null engine");
+    int st = flush_lag(e);
+    if (st) return st;
     CUDA_TRY(cudaStreamSynchronize(e->fft_stream));
     CUDA_TRY(cudaStreamSynchronize(e->stream));
     CUDA_TRY(cudaGetLastError());
@@ -835,6 +872,8 @@ extern "C" int ddm_read_spectrum(ddm_engine *e, int frame, float *out, long capa
 extern "C" int ddm_read_accumulators(ddm_engine *e, double *out, long capacity) {
     clear_error();
     if (!e || !out || capacity < static_cast<long>(e->T * e->E)) return fail(DDM_ERR_INVALID_ARG, "bad argument");
+    int st = flush_lag(e);
+    if (st) return st;
     std::vector<float2> tmp(static_cast<size_t>(e->T) * e->E);
     CUDA_TRY(cudaStreamSynchronize(e->stream));
     CUDA_TRY(cudaMemcpy(tmp.data(), e->acc, sizeof(float2) * tmp.size(), cudaMemcpyDeviceToHost));

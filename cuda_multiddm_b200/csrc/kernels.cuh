@@ -17,7 +17,8 @@ namespace ddm {
 
 constexpr int kMaxScales = 16;
 constexpr int kAzThreads = 256;
-constexpr int kMaxJ = 32;  // frames held in registers by one lag-kernel thread
+constexpr int kMaxJ = 64;          // register frames per element of one lag-kernel launch
+constexpr int kPieceFrames = 32;   // frames per ingest piece (FFT group, staging) at most
 
 struct ScaleDesc {
     int s, tiles;

@@ -2,25 +2,24 @@
 // the partner frame y of every tau, per spectrum element (replaces processFFT,
 // src/DDM_kernel.cuh:85-101, which the reference launches once per (scale, tau, frame)).
 //
-// Work decomposition. One CTA owns a block of kLagBlock consecutive elements of the
-// flattened frame vector (all scales and tiles concatenated, so the kernel needs no
-// geometry). Its threads keep the J register frames of their element in registers. The
-// partner of (register frame j, tau entry e) is window position ub_e + j of a sorted list
-// of distinct partner frames (the "union"), which the host builds per launch: windows of
-// consecutive taus overlap, so a chunk of 30 frames against 64 log-spaced taus up to 500
-// needs about 480 distinct partner frames instead of 30 * 64 = 1920 frame reads.
+// Work decomposition. One CTA owns a block of consecutive elements of the flattened frame
+// vector (all scales and tiles concatenated, so the kernel needs no geometry). Its threads
+// keep the J register frames of their element in registers. The partner of (register
+// frame j, tau entry e) is window position ub_e + j of a sorted list of distinct partner
+// frames (the "union"), which the host builds per launch: windows of consecutive taus
+// overlap, so a chunk of 30 frames against 64 log-spaced taus up to 500 needs 484 distinct
+// partner frames instead of 30 * 64 = 1920 frame reads, and 64 frames need 563.
 //
-// Data movement (sm_100a). Partner frames stream through a ring of kLagSlots shared-memory
-// slots, one slot = the CTA's element block of one frame (1 KB), grouped by kLagGroup. The
-// ring in HBM is addressed through 2-D tensor maps ([slots][elements], boxes of 1..8 slots
-// x kLagBlock elements), so a run of consecutive frames arrives with one
-// cp.async.bulk.tensor.2d (no multicast) that completes on the group's "full" mbarrier. A
-// dedicated producer warp refills a group once every consumer warp has arrived on its
-// "empty" mbarrier, i.e. has moved past the last window that reads it.
-// The ring is a power of two of slots, so a window position becomes a shared-memory address
-// with one add and one mask. The |dF|^2 arithmetic uses packed FP32x2 instructions.
-// Accumulators (FP32 sum + Kahan compensation, 8 B) are loaded three entries ahead with
-// plain coalesced loads and written back once per entry.
+// Data movement (sm_100a). Partner frames stream through a ring of shared-memory slots,
+// one slot = the CTA's element block of one frame, grouped by kLagGroup. The ring in HBM is
+// addressed through 2-D tensor maps ([slots][elements], boxes of 1..8 slots x the CTA's
+// elements), so a run of consecutive frames arrives with one cp.async.bulk.tensor.2d (no
+// multicast) that completes on the group's "full" mbarrier. A dedicated producer warp
+// refills a group once every consumer warp has arrived on its "empty" mbarrier. Consumers
+// wait once per window for every group it reaches, then release the groups no later window
+// reads. The |dF|^2 arithmetic uses packed FP32x2 instructions (FADD2, FFMA2). Accumulators
+// (FP32 sum + Kahan compensation, 8 B) are loaded three entries ahead with plain coalesced
+// loads and written back once per entry.
 //
 // Every mbarrier wait is bounded (kWaitCycles clock cycles); a wait that runs out
 // sets *status to 1, and the CTA waits (bounded again) for its own copies in flight before
@@ -33,26 +32,33 @@
 
 namespace ddm {
 
-constexpr int kLagBlock = 128;                     // elements per CTA, one per consumer thread
-constexpr int kLagConsumerWarps = kLagBlock / 32;
-constexpr int kLagThreads = kLagBlock + 32;        // consumers + one producer warp
-constexpr int kLagSlotsLog2 = 6;
-constexpr int kLagSlots = 1 << kLagSlotsLog2;      // shared-memory frame slots (> 32 frames)
-constexpr uint32_t kLagSlotBytes = kLagBlock * 8;  // one frame of the CTA's elements
-constexpr uint32_t kLagRingBytes = kLagSlots * kLagSlotBytes;
-constexpr uint32_t kLagRingMask = kLagRingBytes - kLagSlotBytes;  // slot bits of a ring offset
+constexpr int kLagConsumerWarps = 4;
+constexpr int kLagThreads = kLagConsumerWarps * 32 + 32;  // consumers + one producer warp
 constexpr int kLagSmemMax = 220 * 1024;
 // Register-frame counts the kernel is instantiated for (a launch uses the smallest >= nreg).
-constexpr int kLagJs[] = {4, 8, 16, 20, 24, 30, 32};
+constexpr int kLagJs[] = {4, 8, 16, 20, 24, 30, 32, 64};
 constexpr int kNumLagJs = sizeof(kLagJs) / sizeof(kLagJs[0]);
+constexpr int kLagMaxJ = 64;
 
 // Union entries are copied in groups of kLagGroup consecutive entries; a group's ring
 // slots arrive as runs of 1, 2, 4 or 8 consecutive slots (one 2-D TMA box each).
 constexpr int kLagGroupLog2 = 3;
 constexpr int kLagGroup = 1 << kLagGroupLog2;
-constexpr int kLagGroupSlotsLog2 = kLagSlotsLog2 - kLagGroupLog2;
-constexpr int kLagGroupSlots = 1 << kLagGroupSlotsLog2;
 constexpr int kLagRunKinds = 4;  // box heights 1, 2, 4, 8
+
+// Geometry of the kernel instantiated for J register frames per element. Up to 32 frames one
+// consumer thread owns an element and holds all J frames in registers; for 64 frames two
+// lanes of a warp (l and l + 16) share an element, each holding 32 frames, and add their
+// pair sums with one shuffle per tau, so the register budget (128 per thread) and three CTAs
+// per SM stay those of 32 frames while the partner reuse is that of 64. A CTA's element
+// block is therefore 128 or 64 elements and a ring slot 1 KB or 512 B. The ring must hold a
+// window plus its alignment, ceil((J - 1) / kLagGroup) + 1 groups, with room to read ahead:
+// 64 slots (8 groups) up to 32 frames, 128 slots (16 groups) for 64; both are 64 KB.
+__host__ __device__ constexpr int lag_lanes(int J) { return J > 32 ? 2 : 1; }
+__host__ __device__ constexpr int lag_cta_elems(int J) { return kLagConsumerWarps * 32 / lag_lanes(J); }
+__host__ __device__ constexpr uint32_t lag_slot_bytes(int J) { return lag_cta_elems(J) * 8u; }
+__host__ __device__ constexpr int lag_ring_slots(int J) { return J > 32 ? 128 : 64; }
+__host__ __device__ constexpr int lag_group_slots(int J) { return lag_ring_slots(J) / kLagGroup; }
 
 // A run: ring slot in bits 0..19, log2(rows) in bits 20..21, position in its group in 22..24.
 __host__ __device__ constexpr int lag_run(int rel, int slot, int log2rows) {
@@ -65,7 +71,7 @@ __host__ __device__ constexpr int lag_run_rel(int run) { return (run >> 22) & 7;
 // Lag table layout (ints): header, register frames, then ntau accumulator indices, ntau
 // union starts, ntau full-window flags, nunion ring slots, ngroups+1 run offsets, nruns runs.
 constexpr int kTabNreg = 0, kTabNtau = 1, kTabNunion = 2, kTabNgroups = 3, kTabNruns = 4, kTabReg = 5;
-constexpr int kTabEntries = kTabReg + 32;
+constexpr int kTabEntries = kTabReg + kLagMaxJ;
 __host__ __device__ constexpr int lag_table_ints(int ntau, int nunion, int ngroups, int nruns) {
     return kTabEntries + 3 * ntau + nunion + ngroups + 1 + nruns;
 }
@@ -124,24 +130,15 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     return true;
 }
 
-// Packed FP32x2 helpers (sm_100a): one instruction for both halves of a complex value.
-__device__ __forceinline__ unsigned long long f2_sub(unsigned long long a, unsigned long long b) {
-    unsigned long long d;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-    return d;
+// Packed FP32x2 arithmetic (sm_100a FADD2 / FFMA2 through the compiler's builtins): one
+// instruction for both halves of a complex value. With the register frames stored negated,
+// d = b + (-r) is exactly -(r - b), so |d|^2 is the pair's |dF|^2 bit for bit.
+__device__ __forceinline__ float2 f2_diff_sq_acc(float2 b, float2 neg_r, float2 acc) {
+    const float2 d = __fadd2_rn(b, neg_r);
+    return __ffma2_rn(d, d, acc);
 }
 
-__device__ __forceinline__ unsigned long long f2_fma_sq(unsigned long long d, unsigned long long acc) {
-    unsigned long long r;
-    asm("fma.rn.f32x2 %0, %1, %1, %2;" : "=l"(r) : "l"(d), "l"(acc));
-    return r;
-}
-
-__device__ __forceinline__ float f2_hsum(unsigned long long v) {
-    return __uint_as_float(static_cast<unsigned>(v)) + __uint_as_float(static_cast<unsigned>(v >> 32));
-}
-
-// 2-D TMA copy of a box of `rows` consecutive ring slots x kLagBlock elements (the box
+// 2-D TMA copy of a box of `rows` consecutive ring slots x a CTA's elements (the box
 // shape is fixed by the tensor map) into shared memory, completing on `bar`.
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar) {
     asm volatile(
@@ -152,27 +149,36 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
 }
 
 // Tensor maps of the ring viewed as a 2-D array [slots][elements] of 8-byte values, with
-// boxes of kLagBlock elements x 1, 2, 4 or 8 slots.
+// boxes of 128 (box[0][*]) or 64 (box[1][*]) elements x 1, 2, 4 or 8 slots.
 struct LagMaps {
-    CUtensorMap box[kLagRunKinds];
+    CUtensorMap box[2][kLagRunKinds];
 };
 
 // Warp-specialised pipeline over groups of kLagGroup union entries. Warps
-// 0..kLagConsumerWarps-1 consume (one spectrum element per thread); the last warp produces
-// (its lane 0 issues the copies). Group g occupies shared-memory slots
-// [(g % groups) * kLagGroup, +kLagGroup); its consecutive ring slots arrive as a few 2-D
-// boxes (runs) that all complete on full[g % groups]; empty[g % groups] completes when every
-// consumer warp has moved past the group. Neither side ever waits for the whole CTA.
+// 0..kLagConsumerWarps-1 consume; the last warp produces (its lane 0 issues the copies).
+// Group g occupies shared-memory slots [(g % kGS) * kLagGroup, +kLagGroup) with
+// kGS = lag_group_slots(J); its consecutive ring slots arrive as a few 2-D boxes (runs) that
+// all complete on full[g % kGS]; empty[g % kGS] completes when every consumer warp has moved
+// past the group. Union entry u therefore sits in shared-memory slot u % lag_ring_slots(J).
+// Neither side ever waits for the whole CTA.
 template <int J>
 __global__ void __launch_bounds__(kLagThreads, 3)
     lag_pipe_kernel(const float2 *__restrict__ ring, float2 *__restrict__ acc, long long E,
                     const int *__restrict__ table, int *__restrict__ status, const __grid_constant__ LagMaps maps) {
+    constexpr int kLanes = lag_lanes(J);
+    constexpr int kJT = J / kLanes;  // register frames per thread
+    constexpr int kElems = lag_cta_elems(J);
+    constexpr uint32_t kSlotBytes = lag_slot_bytes(J);
+    constexpr int kSlots = lag_ring_slots(J);
+    constexpr int kGS = lag_group_slots(J);
+    constexpr uint32_t kRingBytes = kSlots * kSlotBytes;
+    static_assert(J % kLanes == 0 && (kSlots & (kSlots - 1)) == 0 && (kGS & (kGS - 1)) == 0, "lag geometry");
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // ring slots must start on 1 KB boundaries (TMA destinations): align the base at run time
     unsigned char *smem = smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u);
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem + kLagRingBytes);
-    uint64_t *empty = full + kLagGroupSlots;
-    volatile int *abort_flag = reinterpret_cast<volatile int *>(empty + kLagGroupSlots);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + kRingBytes);
+    uint64_t *empty = full + kGS;
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(empty + kGS);
     int *tab = const_cast<int *>(reinterpret_cast<volatile int *>(abort_flag + 1));
 
     const int tid = threadIdx.x;
@@ -180,7 +186,7 @@ __global__ void __launch_bounds__(kLagThreads, 3)
     const int ntab = lag_table_ints(table[kTabNtau], table[kTabNunion], table[kTabNgroups], table[kTabNruns]);
     for (int i = tid; i < ntab; i += kLagThreads) tab[i] = table[i];
     if (tid == 0) {
-        for (int i = 0; i < kLagGroupSlots; i++) {
+        for (int i = 0; i < kGS; i++) {
             mbar_init(&full[i], 1);
             mbar_init(&empty[i], kLagConsumerWarps);
         }
@@ -197,13 +203,13 @@ __global__ void __launch_bounds__(kLagThreads, 3)
     const int *uslot = ent_full + ntau;
     const int *gptr = uslot + nu;
     const int *runs = gptr + ngroups + 1;
-    const long long e0 = static_cast<long long>(blockIdx.x) * kLagBlock;
+    const long long e0 = static_cast<long long>(blockIdx.x) * kElems;
 
     if (warp == kLagConsumerWarps) {
-        // ---------------- producer: group g is fill g / kLagGroupSlots of group slot g % kLagGroupSlots
+        // ---------------- producer: group g is fill g / kGS of group slot g % kGS
         if (lane == 0) {
             for (int g = 0; g < ngroups; g++) {
-                const int gs = g & (kLagGroupSlots - 1), fill = g >> kLagGroupSlotsLog2;
+                const int gs = g & (kGS - 1), fill = g / kGS;
                 if (fill > 0 && !mbar_wait_bounded(&empty[gs], (fill - 1) & 1)) {
                     *abort_flag = 1;
                     break;
@@ -215,93 +221,102 @@ __global__ void __launch_bounds__(kLagThreads, 3)
                     continue;
                 }
                 uint32_t bytes = 0;
-                for (int r = r0; r < r1; r++) bytes += kLagSlotBytes << lag_run_log2rows(runs[r]);
+                for (int r = r0; r < r1; r++) bytes += kSlotBytes << lag_run_log2rows(runs[r]);
                 mbar_expect_tx(&full[gs], bytes);
                 for (int r = r0; r < r1; r++) {
                     const int run = runs[r];
-                    tma_load_2d(smem + (gs * kLagGroup + lag_run_rel(run)) * kLagSlotBytes,
-                                &maps.box[lag_run_log2rows(run)], static_cast<int>(e0), lag_run_slot(run), &full[gs]);
+                    tma_load_2d(smem + (gs * kLagGroup + lag_run_rel(run)) * kSlotBytes,
+                                &maps.box[kLanes - 1][lag_run_log2rows(run)], static_cast<int>(e0), lag_run_slot(run),
+                                &full[gs]);
                 }
             }
         }
     } else {
-        // ---------------- consumers
-        const long long k = e0 + tid;
+        // ---------------- consumers. With two lanes per element, lanes l and l + 16 of a warp
+        // share element l: each half-warp then reads 16 consecutive elements (128 B, every
+        // bank once) of one slot, so a 64-bit shared load stays at two wavefronts.
+        const int h = kLanes == 2 ? (lane >> 4) : 0;
+        const int m = kLanes == 2 ? warp * 16 + (lane & 15) : tid;  // element within the CTA's block
+        const long long k = e0 + m;
         const bool valid = k < E;
-        const uint32_t toff = static_cast<uint32_t>(tid) * sizeof(float2);
-        const unsigned long long *ring64 = reinterpret_cast<const unsigned long long *>(ring);
-        unsigned long long r[J];
+        const uint32_t toff = static_cast<uint32_t>(m) * sizeof(float2);
+        const int j0 = h * kJT;  // first register frame of this thread
+        float2 nr[kJT];          // register frames j0 .. j0 + kJT - 1, negated
 #pragma unroll
-        for (int j = 0; j < J; j++) {
-            const int s = j < nreg ? tab[kTabReg + j] : -1;
-            r[j] = (valid && s >= 0) ? __ldg(ring64 + static_cast<long long>(s) * E + k) : 0ull;
+        for (int i = 0; i < kJT; i++) {
+            const int s = j0 + i < nreg ? tab[kTabReg + j0 + i] : -1;
+            const float2 v = (valid && s >= 0) ? __ldg(ring + static_cast<long long>(s) * E + k) : make_float2(0.f, 0.f);
+            nr[i] = make_float2(-v.x, -v.y);
         }
         const float2 zero = make_float2(0.f, 0.f);
         float2 a0 = (valid && ntau > 0) ? acc[static_cast<long long>(ent_acc[0]) * E + k] : zero;
         float2 a1 = (valid && ntau > 1) ? acc[static_cast<long long>(ent_acc[1]) * E + k] : zero;
         float2 a2 = (valid && ntau > 2) ? acc[static_cast<long long>(ent_acc[2]) * E + k] : zero;
-        int waited = 0, released = 0;  // in groups
+        int waited = 0, released = 0;  // in groups; warp-uniform
         for (int e = 0; e < ntau; e++) {
             const float2 a3 = (valid && e + 3 < ntau) ? acc[static_cast<long long>(ent_acc[e + 3]) * E + k] : zero;
             const int ub = ent_ub[e];
             // Wait for every group this window reaches that no earlier window reached; groups
             // without frames included (they complete by the producer's bare arrival), so a
-            // consumer never releases a group the producer has not issued yet.
+            // consumer never releases a group the producer has not issued yet. One wait per
+            // window keeps the whole window's shared-memory loads free to issue back to back.
             const int glast = (ub + nreg - 1) >> kLagGroupLog2;
             bool ok = true;
-            for (int g = waited; g <= glast; g++) {
-                if (!mbar_wait_bounded(&full[g & (kLagGroupSlots - 1)], (g >> kLagGroupSlotsLog2) & 1)) {
+            for (; waited <= glast; waited++) {
+                if (!mbar_wait_bounded(&full[waited & (kGS - 1)], (waited / kGS) & 1)) {
                     ok = false;
                     break;
                 }
             }
-            if (glast + 1 > waited) waited = glast + 1;
             if (!ok) *abort_flag = 1;
             if (*abort_flag) break;
-            const uint32_t o = static_cast<uint32_t>(ub) * kLagSlotBytes;
-            // four independent packed accumulators (j mod 4) keep the FMA pipeline full
-            unsigned long long acc2[4] = {0ull, 0ull, 0ull, 0ull};
-            const int s0 = ub & (kLagSlots - 1);
-            if (ent_full[e] && s0 + J <= kLagSlots) {
+            const int s0 = ub & (kSlots - 1);
+            // byte offset of this thread's first partner: slot (s0 + j0) of the ring, element m
+            const uint32_t o = static_cast<uint32_t>((s0 + j0) & (kSlots - 1)) * kSlotBytes + toff;
+            // four independent packed accumulators (i mod 4) keep the FMA pipeline full
+            float2 acc2[4] = {zero, zero, zero, zero};
+            if (ent_full[e] && s0 + J <= kSlots) {
                 // whole window present and contiguous in the ring: fixed offsets from one base
-                const unsigned char *w = smem + s0 * kLagSlotBytes + toff;
+                const unsigned char *w = smem + o;
 #pragma unroll
-                for (int j = 0; j < J; j++) {
-                    const unsigned long long b = *reinterpret_cast<const unsigned long long *>(w + j * kLagSlotBytes);
-                    acc2[j & 3] = f2_fma_sq(f2_sub(r[j], b), acc2[j & 3]);
-                }
+                for (int i = 0; i < kJT; i++)
+                    acc2[i & 3] = f2_diff_sq_acc(*reinterpret_cast<const float2 *>(w + i * kSlotBytes), nr[i], acc2[i & 3]);
             } else if (ent_full[e]) {  // nreg == J, every register frame and partner present
 #pragma unroll
-                for (int j = 0; j < J; j++) {
-                    const uint32_t off = ((o + j * kLagSlotBytes) & kLagRingMask) | toff;
-                    const unsigned long long b = *reinterpret_cast<const unsigned long long *>(smem + off);
-                    acc2[j & 3] = f2_fma_sq(f2_sub(r[j], b), acc2[j & 3]);
+                for (int i = 0; i < kJT; i++) {
+                    const uint32_t off = (o + i * kSlotBytes) & (kRingBytes - 1);  // toff < kSlotBytes survives the mask
+                    acc2[i & 3] = f2_diff_sq_acc(*reinterpret_cast<const float2 *>(smem + off), nr[i], acc2[i & 3]);
                 }
             } else {
 #pragma unroll
-                for (int j = 0; j < J; j++) {
+                for (int i = 0; i < kJT; i++) {
+                    const int j = j0 + i;
                     if (j < nreg && tab[kTabReg + j] >= 0 && uslot[ub + j] >= 0) {
-                        const uint32_t off = ((o + j * kLagSlotBytes) & kLagRingMask) | toff;
-                        const unsigned long long b = *reinterpret_cast<const unsigned long long *>(smem + off);
-                        acc2[j & 3] = f2_fma_sq(f2_sub(r[j], b), acc2[j & 3]);
+                        const uint32_t off = (o + i * kSlotBytes) & (kRingBytes - 1);
+                        acc2[i & 3] = f2_diff_sq_acc(*reinterpret_cast<const float2 *>(smem + off), nr[i], acc2[i & 3]);
                     }
                 }
             }
-            const float sum = (f2_hsum(acc2[0]) + f2_hsum(acc2[1])) + (f2_hsum(acc2[2]) + f2_hsum(acc2[3]));
+            float sum = ((acc2[0].x + acc2[0].y) + (acc2[1].x + acc2[1].y)) +
+                        ((acc2[2].x + acc2[2].y) + (acc2[3].x + acc2[3].y));
+            if (kLanes == 2) sum += __shfl_xor_sync(0xffffffffu, sum, 16);  // same value in both lanes
             // Kahan step: a.x running sum, a.y compensation (true value a.x - a.y)
             const float y = sum - a0.y;
             const float t = a0.x + y;
             a0.y = (t - a0.x) - y;
             a0.x = t;
-            if (valid) acc[static_cast<long long>(ent_acc[e]) * E + k] = a0;
+            if (valid && h == 0) acc[static_cast<long long>(ent_acc[e]) * E + k] = a0;
             a0 = a1;
             a1 = a2;
             a2 = a3;
             // release the groups no later window reads (all their entries lie below the next window)
-            const int next_g = (e + 1 < ntau ? ent_ub[e + 1] : nu) >> kLagGroupLog2;
-            __syncwarp();
-            if (lane == 0)
-                for (; released < next_g; released++) mbar_arrive(&empty[released & (kLagGroupSlots - 1)]);
+            const int rel = (e + 1 < ntau ? ent_ub[e + 1] : nu) >> kLagGroupLog2;
+            if (rel > released) {
+                __syncwarp();
+                if (lane == 0)
+                    for (int g = released; g < rel; g++) mbar_arrive(&empty[g & (kGS - 1)]);
+                released = rel;
+            }
         }
     }
     __syncthreads();
@@ -309,10 +324,10 @@ __global__ void __launch_bounds__(kLagThreads, 3)
         if (tid == 0) {
             atomicExch(status, 1);
             // drain: wait (bounded) until every copy this CTA issued has landed
-            for (int gs = 0; gs < kLagGroupSlots; gs++) {
-                for (int g = gs; g < ngroups; g += kLagGroupSlots) {
-                    if (!mbar_try_wait(&full[gs], (g >> kLagGroupSlotsLog2) & 1)) {
-                        mbar_wait_bounded(&full[gs], (g >> kLagGroupSlotsLog2) & 1);
+            for (int gs = 0; gs < kGS; gs++) {
+                for (int g = gs; g < ngroups; g += kGS) {
+                    if (!mbar_try_wait(&full[gs], (g / kGS) & 1)) {
+                        mbar_wait_bounded(&full[gs], (g / kGS) & 1);
                         break;
                     }
                 }
@@ -322,8 +337,11 @@ __global__ void __launch_bounds__(kLagThreads, 3)
     }
 }
 
-inline size_t lag_smem_bytes(int table_ints) {
-    return 1024 + kLagRingBytes + 2 * sizeof(uint64_t) * kLagGroupSlots + sizeof(int) * (1 + table_ints);
+// Dynamic shared memory of a launch of lag_pipe_kernel<J> with a table of table_ints ints
+// (1 KB of alignment slack, ring, barriers, abort flag, table).
+inline size_t lag_smem_bytes(int J, int table_ints) {
+    return 1024 + static_cast<size_t>(lag_ring_slots(J)) * lag_slot_bytes(J) + 2 * sizeof(uint64_t) * lag_group_slots(J) +
+           sizeof(int) * (1 + table_ints);
 }
 
 }  // namespace ddm

@@ -26,6 +26,7 @@ namespace ddm {
 inline std::string build_lag_table(int nreg, const int *reg, const std::vector<int> &ent_acc,
                                    const std::vector<int> &ent_w, const std::vector<int> &pos, int J,
                                    std::vector<int> *table) {
+    if (nreg < 1 || nreg > J || J > kLagMaxJ) return "register frame count out of range";
     const int ntau = static_cast<int>(ent_acc.size());
     std::vector<int> ub(ntau), uslot;
     uslot.reserve(pos.size());
@@ -77,7 +78,7 @@ inline std::string build_lag_table(int nreg, const int *reg, const std::vector<i
     t[kTabNunion] = nu;
     t[kTabNgroups] = ngroups;
     t[kTabNruns] = nruns;
-    for (int j = 0; j < 32; j++) t[kTabReg + j] = j < nreg ? reg[j] : -1;
+    for (int j = 0; j < kLagMaxJ; j++) t[kTabReg + j] = j < nreg ? reg[j] : -1;
     int *p = t + kTabEntries;
     p = std::copy(ent_acc.begin(), ent_acc.end(), p);
     p = std::copy(ub.begin(), ub.end(), p);
@@ -101,7 +102,8 @@ inline int lag_pick_j(int nreg) {
     return 0;
 }
 
-// Tensor maps of a ring float2[slots][E] for boxes of kLagBlock elements x 1, 2, 4, 8 slots.
+// Tensor maps of a ring float2[slots][E] for boxes of 128 or 64 elements (the element blocks
+// of the one- and two-lane kernels) x 1, 2, 4, 8 slots.
 inline std::string make_lag_maps(const void *ring, long long E, int slots, LagMaps *maps) {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if (!encode) {
@@ -116,12 +118,16 @@ inline std::string make_lag_maps(const void *ring, long long E, int slots, LagMa
     const cuuint64_t dims[2] = {static_cast<cuuint64_t>(E), static_cast<cuuint64_t>(slots)};
     const cuuint64_t strides[1] = {static_cast<cuuint64_t>(E) * 8};
     const cuuint32_t estr[2] = {1, 1};
-    for (int k = 0; k < kLagRunKinds; k++) {
-        const cuuint32_t box[2] = {static_cast<cuuint32_t>(kLagBlock), 1u << k};
-        CUresult r = encode(&maps->box[k], CU_TENSOR_MAP_DATA_TYPE_INT64, 2, const_cast<void *>(ring), dims, strides, box,
-                            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-        if (r != CUDA_SUCCESS) return "cuTensorMapEncodeTiled failed with code " + std::to_string(static_cast<int>(r));
+    const int widths[2] = {lag_cta_elems(1), lag_cta_elems(kLagMaxJ)};
+    for (int w = 0; w < 2; w++) {
+        for (int k = 0; k < kLagRunKinds; k++) {
+            const cuuint32_t box[2] = {static_cast<cuuint32_t>(widths[w]), 1u << k};
+            CUresult r = encode(&maps->box[w][k], CU_TENSOR_MAP_DATA_TYPE_INT64, 2, const_cast<void *>(ring), dims,
+                                strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS)
+                return "cuTensorMapEncodeTiled failed with code " + std::to_string(static_cast<int>(r));
+        }
     }
     return std::string();
 }

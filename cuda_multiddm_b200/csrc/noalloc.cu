@@ -127,8 +127,8 @@ extern "C" int ddm_lag_accumulate_static(const void *ring, int ring_slots, long 
     cudaError_t ce = cudaMemcpyAsync(d_table, table.data(), sizeof(int) * table.size(), cudaMemcpyHostToDevice, s);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(d_status, 0, sizeof(int), s);
     if (ce != cudaSuccess) return fail(DDM_ERR_CUDA, std::string("ddm_lag_accumulate_static: ") + cudaGetErrorString(ce));
-    const unsigned blocks = static_cast<unsigned>((elements + kLagBlock - 1) / kLagBlock);
-    const size_t smem = lag_smem_bytes(static_cast<int>(table.size()));
+    const unsigned blocks = static_cast<unsigned>((elements + lag_cta_elems(J) - 1) / lag_cta_elems(J));
+    const size_t smem = lag_smem_bytes(J, static_cast<int>(table.size()));
     const float2 *r = static_cast<const float2 *>(ring);
     float2 *a = static_cast<float2 *>(acc);
     switch (J) {

@@ -33,6 +33,7 @@ class EngineConfig:
     hbm_budget_bytes: int = 0
     device: int = 0
     stream: int | None = None          # a cudaStream_t as an integer, or None
+    lag_batch_frames: int = 0          # frames per lag launch (1..64; 0 = min(chunk_frames, 32))
     _keep: list = field(default_factory=list, repr=False)
 
     def to_c(self) -> Config:
@@ -46,7 +47,7 @@ class EngineConfig:
                       self.y_offset, sc, len(self.scales), ta, len(self.taus), la, len(self.lambdas),
                       C.c_float(self.tolerance), self.chunk_frames, est, int(bool(self.multistream)),
                       self.total_frames, self.dump_every, self.hbm_budget_bytes, self.device,
-                      C.c_void_p(self.stream) if self.stream else None)
+                      C.c_void_p(self.stream) if self.stream else None, self.lag_batch_frames)
 
 
 def isf_blocks(isf: np.ndarray, scales: Sequence[int], n_lambda: int, n_tau: int) -> dict:

@@ -73,6 +73,10 @@ typedef struct {
     size_t hbm_budget_bytes;       /* refuse to open if the engine would need more; 0 = no limit */
     int device;                    /* CUDA device ordinal */
     void *stream;                  /* cudaStream_t to run on; NULL = the engine creates one */
+    int lag_batch_frames;          /* frames paired per lag launch, 1..64; 0 = min(C, 32),
+                                      one launch per ingest piece. Unbiased: a larger value
+                                      holds frames back for fuller launches, which read fewer
+                                      partner bytes per frame. Compat: A-frames per launch. */
 } ddm_config;
 
 typedef struct ddm_engine ddm_engine;
@@ -89,10 +93,13 @@ int ddm_close(ddm_engine *e);
 /* Submit `count` consecutive source frames, each frame_height rows of
  * frame_width*bytes_per_pixel bytes, rows packed. `on_device` = 0: host memory (pinned
  * memory gives asynchronous copies); 1: device memory on the engine's device, read in
- * place. Frames are transformed into the ring and every lag pair that becomes complete
- * is accumulated. Replaces the chunk loop of runDDM (src/DDM.cu:765-843: H2D copy :767,
- * parseChunk :154 -> parseBufferScalePow2 + cufftExecR2C, analyseChunk :222 ->
- * processFFT). Returns once the work is queued on the engine's stream. */
+ * place. Frames are transformed into the ring and their lag pairs are accumulated; with
+ * the unbiased estimator the lag work of up to lag_batch_frames - 1 frames may be held back
+ * for a fuller launch, and ddm_finalize, ddm_synchronize, ddm_reset_accumulators and
+ * ddm_read_accumulators queue it first. Replaces the chunk loop of runDDM
+ * (src/DDM.cu:765-843: H2D copy :767, parseChunk :154 -> parseBufferScalePow2 +
+ * cufftExecR2C, analyseChunk :222 -> processFFT). Returns once the work is queued on the
+ * engine's stream. */
 int ddm_submit_frames(ddm_engine *e, const void *frames, int count, int on_device);
 
 /* Queue the remaining pairs (compat tail, src/DDM.cu:830-843) and the masked azimuthal

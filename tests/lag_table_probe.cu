@@ -13,7 +13,7 @@
 int main() {
     int nreg, J, ntau, npos;
     while (std::cin >> nreg >> J >> ntau >> npos) {
-        std::vector<int> reg(32, -1), ent_acc(ntau), ent_w(ntau), pos(npos);
+        std::vector<int> reg(64, -1), ent_acc(ntau), ent_w(ntau), pos(npos);
         for (int j = 0; j < nreg; j++) std::cin >> reg[j];
         for (int &v : ent_acc) std::cin >> v;
         for (int &v : ent_w) std::cin >> v;

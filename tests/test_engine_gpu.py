@@ -32,14 +32,15 @@ def assert_isf_close(got, want, scales, Q, T, rtol=RTOL):
 
 
 def engine_run(frames, scales, taus, lambdas, *, estimator, N=None, C=10, tol=1.2, multistream=True, G=0,
-               x_off=0, y_off=0, pixel_mode="byte0", on_device=False):
+               x_off=0, y_off=0, pixel_mode="byte0", on_device=False, lag_batch=0):
     n, h, w = frames.shape[:3]
     bpp = 2 if frames.dtype == np.uint16 else 1
     raw = np.ascontiguousarray(frames).view(np.uint8).reshape(n, h, w * bpp)
     N = n if N is None else N
     cfg = EngineConfig(frame_width=w, frame_height=h, scales=scales, taus=taus, lambdas=lambdas, tolerance=tol,
                        chunk_frames=C, estimator=estimator, total_frames=N, multistream=multistream, dump_every=G,
-                       bytes_per_pixel=bpp, pixel_mode=pixel_mode, x_offset=x_off, y_offset=y_off)
+                       bytes_per_pixel=bpp, pixel_mode=pixel_mode, x_offset=x_off, y_offset=y_off,
+                       lag_batch_frames=lag_batch)
     with Engine(cfg) as eng:
         need = eng.info().frames_needed if estimator == "compat" else N
         if on_device:
@@ -144,6 +145,56 @@ def test_chunking_does_not_change_unbiased_result():
     a, _, _ = engine_run(frames, *args, estimator="unbiased", C=5)
     b, _, _ = engine_run(frames, *args, estimator="unbiased", C=32)
     assert_isf_close(a, b, [64, 32], 3, 5, rtol=2e-6)
+
+
+def test_full_lag_launches_match_oracle():
+    """lag_batch_frames = 64 with 200 frames in 30-frame pieces: three full 64-frame lag
+    launches (the two-lane kernel, windows that wrap its shared-memory ring and windows that
+    do not) and an 8-frame launch at finalize; once against the oracle, once with a finalize
+    after every piece (each flushes the held-back frames into smaller launches) against the
+    first result."""
+    frames = media.synth_video(41, 128, 128, 200, 80, step_var=1.0)
+    scales, taus, lambdas = [128, 64], media.log_taus(1, 150, 24), [2.5, 5.0, 9.0, 17.0, 33.0]
+    isf, _, info = engine_run(frames, scales, taus, lambdas, estimator="unbiased", C=30, lag_batch=64)
+    want, _ = O.ddm_run(frames, scales, taus, lambdas, estimator=O.EST_UNBIASED, chunk=30)
+    assert_isf_close(isf, want, scales, len(lambdas), len(taus))
+    assert info.ring_slots == 150 + 2 * 30 + 63
+    cfg = EngineConfig(frame_width=128, frame_height=128, scales=scales, taus=taus, lambdas=lambdas,
+                       chunk_frames=30, estimator="unbiased", lag_batch_frames=64)
+    with Engine(cfg) as eng:
+        for c0 in range(0, 200, 30):
+            eng.submit(frames[c0:c0 + 30])
+            eng.finalize()
+        live = eng.isf()
+    assert_isf_close(live, isf, scales, len(lambdas), len(taus), rtol=2e-6)
+
+
+def test_lag_batch_sizes_agree():
+    """The same stream paired in launches of 1, 13, 30 and 64 frames gives the same ISF."""
+    frames = media.synth_video(44, 64, 64, 90, 30, step_var=1.0)
+    scales, taus, lambdas = [64, 32], [1, 2, 4, 8, 17, 33], [3.0, 6.0, 12.0]
+    out = []
+    for lb in (1, 13, 30, 64):
+        cfg = EngineConfig(frame_width=64, frame_height=64, scales=scales, taus=taus, lambdas=lambdas,
+                           chunk_frames=10, estimator="unbiased", lag_batch_frames=lb)
+        with Engine(cfg) as eng:
+            eng.submit(frames)
+            eng.finalize()
+            out.append(eng.isf())
+    for o in out[1:]:
+        assert_isf_close(o, out[0], scales, len(lambdas), len(taus), rtol=2e-6)
+
+
+def test_compat_long_chunk_matches_oracle():
+    """C = 100 with lag_batch_frames = 64: each reference iteration pairs 100 A-frames, run as
+    a 64-frame launch and a 36-frame launch of the 64-frame kernel (the partial-window path);
+    with the default, as launches of 32, 32, 32 and 4."""
+    frames = media.synth_video(43, 64, 64, 200, 30, step_var=1.0)
+    scales, taus, lambdas = [64, 32], [1, 2, 5, 13, 40, 99], [3.0, 6.0, 12.0, 24.0]
+    want, _ = O.ddm_run(frames, scales, taus, lambdas, estimator=O.EST_COMPAT, chunk=100)
+    for lb in (64, 0):
+        isf, _, _ = engine_run(frames, scales, taus, lambdas, estimator="compat", C=100, lag_batch=lb)
+        assert_isf_close(isf, want, scales, len(lambdas), len(taus))
 
 
 def test_errors_are_status_codes():

@@ -1,10 +1,10 @@
 """CPU checks of the lag kernel's launch tables and its shared-memory pipeline protocol.
 
 The lag kernel (cuda_multiddm_b200/csrc/lag.cuh) streams the distinct partner frames of a
-launch (the "union") through 8 groups of 8 shared-memory slots: one producer lane issues
-each group's 2-D TMA boxes and arms the group's *full* barrier; four consumer warps wait on
-every group their window reaches and arrive on the group's *empty* barrier once no later
-window reads it. These tests build the tables with the engine's own C++ builder
+launch (the "union") through groups of 8 shared-memory slots (8 groups for up to 32
+register frames, 16 for 64): one producer lane issues each group's 2-D TMA boxes and arms
+the group's *full* barrier; four consumer warps wait once per window on every group it
+reaches and arrive on a group's *empty* barrier once no later window reads it. These tests build the tables with the engine's own C++ builder
 (``build_lag_table``, csrc/lag_host.hpp, driven by tests/lag_table_probe.cu) for the
 schedules the engine launches — causal windows (unbiased estimator) and the reference's
 start|end windows (src/DDM.cu:250-255) — plus random windows with holes, and check
@@ -21,6 +21,7 @@ from __future__ import annotations
 
 import random
 import subprocess
+import sys
 from pathlib import Path
 
 import pytest
@@ -33,10 +34,18 @@ PROBE_SRC = ROOT / "tests" / "lag_table_probe.cu"
 PROBE = ROOT / "tests" / "_build" / "lag_table_probe"
 
 # constants of csrc/lag.cuh
-SLOTS, GROUP, GROUP_SLOTS, CONSUMERS = 64, 8, 8, 4
-LAG_JS = (4, 8, 16, 20, 24, 30, 32)
-SLOT_BYTES, SMEM_MAX = 1024, 220 * 1024
-TAB_ENTRIES = 5 + 32
+GROUP, CONSUMERS = 8, 4
+LAG_JS = (4, 8, 16, 20, 24, 30, 32, 64)
+SMEM_MAX = 220 * 1024
+TAB_ENTRIES = 5 + 64
+
+
+def ring_slots(J: int) -> int:
+    return 128 if J > 32 else 64
+
+
+def slot_bytes(J: int) -> int:
+    return 512 if J > 32 else 1024  # a CTA's element block: 64 (two lanes each) or 128 elements
 
 
 def pick_j(nreg: int) -> int:
@@ -69,7 +78,7 @@ def build_tables(probe: Path, cases: list[dict]) -> list[list[int] | str]:
 def parse(t: list[int]) -> dict:
     nreg, ntau, nu, ngroups, nruns = t[:5]
     p = TAB_ENTRIES
-    d = {"nreg": nreg, "ntau": ntau, "nu": nu, "ngroups": ngroups, "reg": t[5:5 + 32]}
+    d = {"nreg": nreg, "ntau": ntau, "nu": nu, "ngroups": ngroups, "reg": t[5:5 + 64]}
     for name, n in (("ent_acc", ntau), ("ub", ntau), ("full", ntau), ("uslot", nu),
                     ("gptr", ngroups + 1), ("runs", nruns)):
         d[name] = t[p:p + n]
@@ -95,7 +104,7 @@ def causal_case(taus: list[int], n0: int, c: int, R: int) -> dict:
 def compat_case(taus: list[int], start: list[int], end: list[int], f0: int, R: int) -> dict:
     """lag_iteration: A = start[f0..], partner of position q = start|end[q]."""
     C = len(start)
-    nreg = min(32, C - f0)
+    nreg = min(64, C - f0)
     slot = lambda f: f % R if f >= 0 else -1  # noqa: E731
     pos = []
     for p in range(nreg + max(taus)):
@@ -107,7 +116,7 @@ def compat_case(taus: list[int], start: list[int], end: list[int], f0: int, R: i
 
 
 def random_case(rnd: random.Random) -> dict:
-    nreg = rnd.choice([1, 3, 4, 7, 8, 16, 20, 29, 30, 32])
+    nreg = rnd.choice([1, 3, 4, 7, 8, 16, 20, 29, 30, 32, 33, 50, 63, 64])
     ntau = rnd.randint(1, 70)
     starts = sorted(rnd.sample(range(0, 600), ntau))
     npos = starts[-1] + nreg
@@ -125,17 +134,18 @@ def schedule_cases() -> list[dict]:
     tau_sets = [log_taus(1, 500, 64), [1, 2, 3, 5, 8, 13, 21, 34, 55], list(range(1, 21)),
                 log_taus(1, 300, 48), [1], [7, 300]]
     for taus in tau_sets:
-        for c in (30, 32, 20, 8, 1, 3):
-            R = max(taus) + 2 * c
+        for c in (30, 32, 20, 8, 1, 3, 64, 60, 45):
+            R = max(taus) + 63 + 2 * min(c, 64)
             for n0 in (0, 7, 30, 200, 600, 1000):
                 cases.append(causal_case(taus, n0, c, R))
-    for taus, C in ((list(range(1, 21)), 20), ([1, 2, 4, 8, 16, 32], 40), ([1, 3, 9], 10), ([2, 5], 64)):
+    for taus, C in ((list(range(1, 21)), 20), ([1, 2, 4, 8, 16, 32], 40), ([1, 3, 9], 10), ([2, 5], 64),
+                    (log_taus(1, 500, 64), 500)):
         R = 3 * C + 5
         for base in (0, 7 * C):
             start = [base + i for i in range(C)]
             for end in ([base + C + i for i in range(C)], [-1] * C,            # tail: nothing yet
                         [base + 2 * C + i for i in range(C)]):                 # stale pinned buffer
-                for f0 in range(0, C, 32):
+                for f0 in range(0, C, 64):
                     cases.append(compat_case(taus, start, end, f0, R))
     rnd = random.Random(1234)
     cases += [random_case(rnd) for _ in range(150)]
@@ -176,7 +186,8 @@ def check_table(case: dict, d: dict) -> None:
                 seen.add(u)
     assert seen == {u for u in range(nu) if us[u] >= 0}
     ntab = TAB_ENTRIES + 3 * d["ntau"] + nu + d["ngroups"] + 1 + len(d["runs"])
-    assert 1024 + SLOTS * SLOT_BYTES + 2 * 8 * GROUP_SLOTS + 4 * (1 + ntab) <= SMEM_MAX
+    slots = ring_slots(J)
+    assert 1024 + slots * slot_bytes(J) + 2 * 8 * (slots // GROUP) + 4 * (1 + ntab) <= SMEM_MAX
 
 
 def parity_done(completed: int, parity: int) -> bool:
@@ -184,12 +195,17 @@ def parity_done(completed: int, parity: int) -> bool:
     return completed >= 1 and (completed - 1) % 2 == parity
 
 
-def replay(d: dict, seed: int) -> str:
-    """Random interleaving of the producer lane and the consumer warps, as lag_pipe_kernel."""
+def replay(d: dict, seed: int, skip_empty_waits: bool = False) -> str:
+    """Random interleaving of the producer lane and the consumer warps, as lag_pipe_kernel:
+    a consumer waits once per window for every group up to the window's last, reads the
+    window, then releases the groups below the next window. ``skip_empty_waits`` plants the
+    protocol error the kernel avoids (not waiting on groups without frames)."""
     rnd = random.Random(seed)
     nreg, ntau, nu, ngroups, ub = d["nreg"], d["ntau"], d["nu"], d["ngroups"], d["ub"]
-    full_c, empty_c, empty_arr = [0] * GROUP_SLOTS, [0] * GROUP_SLOTS, [0] * GROUP_SLOTS
-    content = [None] * GROUP_SLOTS  # which group a group slot holds
+    gslots = ring_slots(pick_j(nreg)) // GROUP
+    empty_groups = {g for g in range(ngroups) if d["gptr"][g] == d["gptr"][g + 1]}
+    full_c, empty_c, empty_arr = [0] * gslots, [0] * gslots, [0] * gslots
+    content = [None] * gslots  # which group a group slot holds
     g_next = 0
     warps = [{"e": 0, "waited": 0, "released": 0} for _ in range(CONSUMERS)]
     idle = 0
@@ -200,7 +216,7 @@ def replay(d: dict, seed: int) -> str:
         a = rnd.choice(actors)
         progressed = False
         if a == "P":
-            gs, fill = g_next % GROUP_SLOTS, g_next // GROUP_SLOTS
+            gs, fill = g_next % gslots, g_next // gslots
             if fill == 0 or parity_done(empty_c[gs], (fill - 1) & 1):
                 full_c[gs] += 1  # data landed (or bare arrive for a group without frames)
                 content[gs] = g_next
@@ -210,20 +226,21 @@ def replay(d: dict, seed: int) -> str:
             s = warps[a]
             e = s["e"]
             glast = (ub[e] + nreg - 1) // GROUP
-            if all(parity_done(full_c[g % GROUP_SLOTS], (g // GROUP_SLOTS) & 1) for g in range(s["waited"], glast + 1)):
+            need = [g for g in range(s["waited"], glast + 1) if not (skip_empty_waits and g in empty_groups)]
+            if all(parity_done(full_c[g % gslots], (g // gslots) & 1) for g in need):
                 s["waited"] = max(s["waited"], glast + 1)
                 for j in range(nreg):
                     u = ub[e] + j
-                    if d["uslot"][u] >= 0 and content[(u // GROUP) % GROUP_SLOTS] != u // GROUP:
+                    if d["uslot"][u] >= 0 and d["reg"][j] >= 0 and content[(u // GROUP) % gslots] != u // GROUP:
                         return f"stale read of union entry {u} by entry {e}"
-                next_g = (ub[e + 1] if e + 1 < ntau else nu) // GROUP
-                for g in range(s["released"], next_g):
-                    gs = g % GROUP_SLOTS
+                upto = (ub[e + 1] if e + 1 < ntau else nu) // GROUP
+                for g in range(s["released"], upto):
+                    gs = g % gslots
                     empty_arr[gs] += 1
                     if empty_arr[gs] == CONSUMERS:
                         empty_arr[gs] = 0
                         empty_c[gs] += 1
-                s["released"] = max(s["released"], next_g)
+                s["released"] = max(s["released"], upto)
                 s["e"] += 1
                 progressed = True
         idle = 0 if progressed else idle + 1
@@ -261,57 +278,19 @@ def test_union_shrinks_reads():
 
 def test_wrong_protocol_is_caught(probe):
     """The replay catches a consumer that skips waiting on groups without frames (the
-    protocol error the kernel avoids): with it the consumer may release a group slot before
-    the producer has filled it, which shows up as a stale read or a deadlock."""
-    d = parse(build_tables(probe, [causal_case(log_taus(1, 500, 64), 0, 30, 560)])[0])
-    bad = dict(d)
-    # plant the mistake in the model: groups without frames count as already waited on
-    empty_groups = [g for g in range(d["ngroups"]) if d["gptr"][g] == d["gptr"][g + 1]]
-    assert empty_groups, "the case must have groups without frames"
+    protocol error the kernel avoids): it may then release a group slot before the producer
+    has filled it, which shows up as a stale read or a deadlock."""
+    for c in (30, 64):
+        d = parse(build_tables(probe, [causal_case(log_taus(1, 500, 64), 0, c, 700)])[0])
+        assert any(d["gptr"][g] == d["gptr"][g + 1] for g in range(d["ngroups"])), "needs frame-less groups"
+        assert any(replay(d, seed, skip_empty_waits=True) != "ok" for seed in range(20))
+        assert all(replay(d, seed) == "ok" for seed in range(20))
 
-    def replay_skip(seed: int) -> str:
-        rnd = random.Random(seed)
-        nreg, ntau, nu, ngroups, ub = bad["nreg"], bad["ntau"], bad["nu"], bad["ngroups"], bad["ub"]
-        full_c, empty_c, empty_arr = [0] * GROUP_SLOTS, [0] * GROUP_SLOTS, [0] * GROUP_SLOTS
-        content = [None] * GROUP_SLOTS
-        g_next, idle = 0, 0
-        warps = [{"e": 0, "released": 0} for _ in range(CONSUMERS)]
-        while True:
-            actors = (["P"] if g_next < ngroups else []) + [w for w in range(CONSUMERS) if warps[w]["e"] < ntau]
-            if not actors:
-                return "ok"
-            a = rnd.choice(actors)
-            progressed = False
-            if a == "P":
-                gs, fill = g_next % GROUP_SLOTS, g_next // GROUP_SLOTS
-                if fill == 0 or parity_done(empty_c[gs], (fill - 1) & 1):
-                    full_c[gs] += 1
-                    content[gs] = g_next
-                    g_next += 1
-                    progressed = True
-            else:
-                s = warps[a]
-                e = s["e"]
-                glast = (ub[e] + nreg - 1) // GROUP
-                need = [g for g in range(ub[e] // GROUP, glast + 1) if g not in empty_groups]
-                if all(parity_done(full_c[g % GROUP_SLOTS], (g // GROUP_SLOTS) & 1) for g in need):
-                    for j in range(nreg):
-                        u = ub[e] + j
-                        if bad["uslot"][u] >= 0 and content[(u // GROUP) % GROUP_SLOTS] != u // GROUP:
-                            return "stale"
-                    next_g = (ub[e + 1] if e + 1 < ntau else nu) // GROUP
-                    for g in range(s["released"], next_g):
-                        gs = g % GROUP_SLOTS
-                        empty_arr[gs] += 1
-                        if empty_arr[gs] == CONSUMERS:
-                            empty_arr[gs] = 0
-                            empty_c[gs] += 1
-                    s["released"] = max(s["released"], next_g)
-                    s["e"] += 1
-                    progressed = True
-            idle = 0 if progressed else idle + 1
-            if idle > 4000:
-                return "deadlock"
 
-    assert any(replay_skip(seed) != "ok" for seed in range(20))
-    assert all(replay(d, seed) == "ok" for seed in range(20))
+def test_ring_must_hold_a_full_window(probe, monkeypatch):
+    """With 64 register frames a 64-slot ring cannot hold a window and the group the next
+    window shares with it: the replay deadlocks, which is why that kernel has 128 slots."""
+    d = parse(build_tables(probe, [causal_case(list(range(1, 21)), 200, 64, 200)])[0])
+    assert replay(d, 0) == "ok"
+    monkeypatch.setattr(sys.modules[__name__], "ring_slots", lambda J: 64)
+    assert replay(d, 0) == "deadlock"
