@@ -67,6 +67,8 @@ SIGNATURES = {
     "ddm_frame_elements": (C.c_long, [C.c_void_p]),
     "ddm_read_spectrum": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_long]),
     "ddm_read_accumulators": (C.c_int, [C.c_void_p, C.c_void_p, C.c_long]),
+    "ddm_read_power_spectrum": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_long]),
+    "ddm_read_unaveraged": (C.c_int, [C.c_void_p, C.c_void_p, C.c_long]),
     "ddm_get_info": (C.c_int, [C.c_void_p, C.POINTER(Info)]),
     "ddm_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
     "ddm_kernel_times": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -8,8 +8,10 @@
 //   -f PATH -M                              .movie input (-f without -M needs OpenCV: unavailable)
 //   -B ARG                                  benchmark mode on random frames (takes an argument,
 //                                           as in the reference)
-//   -s -x -y -I -v -Z -t -C -G -F -K -A -W  as in the reference; -F is accepted and, like the
-//                                           reference, has no effect; -K/-A/-W are refused
+//   -s -x -y -I -v -Z -t -C -G -F -W        as in the reference; -F is accepted and, like the
+//                                           reference, has no effect; -W is refused
+//   -K ARG -A                               the reference's debug outputs, with corrected
+//                                           contents (see write_unaveraged / write_power)
 // Flags added here:
 //   -E compat|unbiased   estimator (default compat: the reference's own pairing)
 //   -P byte0|u16         16-bit pixel decoding (default byte0: the reference's first byte)
@@ -66,9 +68,84 @@ void print_help() {
                  "  -C INT       frames per chunk (default 100)\n"
                  "  -G INT       write and reset the ISF every INT chunks\n"
                  "  -F FPS       accepted, no effect (as in the reference)\n"
+                 "  -K ARG       also write <PATH><scale>-<tile>-nonAve: per tau, the structure\n"
+                 "               function of every wave vector before the azimuthal average\n"
+                 "  -A           also write <PATH>_fft_chunk_<k>-<scale>: |F/s^2|^2 of every\n"
+                 "               frame and tile of chunk k\n"
                  "  -E MODE      compat (default) or unbiased estimator\n"
                  "  -P MODE      byte0 (default) or u16 decoding of 16-bit pixels\n");
 }
+
+// Number text as std::ostream prints a float (6 significant digits), then one space, as
+// the reference's writers do (src/azimuthal_average.cu:31-150).
+inline void put_value(FILE *f, double v) { std::fprintf(f, "%g ", static_cast<double>(static_cast<float>(v))); }
+
+FILE *open_out(const std::string &name) {
+    FILE *f = std::fopen(name.c_str(), "w");
+    if (!f) {
+        std::fprintf(stderr, "[Out Error] Unable to open %s.\n", name.c_str());
+        std::exit(EXIT_FAILURE);
+    }
+    return f;
+}
+
+// -K: <prefix><scale>-<tile>-nonAve (file name of src/DDM.cu:120). Header lines as the ISF
+// file (lambdas, tau / fps); then one line per tau with the tile's s*(s/2+1) values of
+// 2 * mean|dF|^2 / s^4 in [ky][kx] order, whose mean over an annulus mask is that ISF bin.
+// (The reference's rows use a row stride of tau_count instead of the tile size and the
+// accumulator tile offset of src/DDM.cu:122; this writes what those rows were meant to hold.)
+void write_unaveraged(const std::string &prefix, const std::vector<double> &unav, long E,
+                      const std::vector<int> &scales, const std::vector<float> &lambdas,
+                      const std::vector<int> &taus, float fps) {
+    long off = 0;
+    for (int s : scales) {
+        const int tiles = (scales[0] / s) * (scales[0] / s);
+        const long n = static_cast<long>(s) * (s / 2 + 1);
+        for (int tile = 0; tile < tiles; tile++, off += n) {
+            FILE *f = open_out(prefix + std::to_string(s) + "-" + std::to_string(tile) + "-nonAve");
+            for (float l : lambdas) put_value(f, l);
+            std::fputc('\n', f);
+            for (int t : taus) put_value(f, static_cast<float>(t) / fps);
+            std::fputc('\n', f);
+            for (size_t ti = 0; ti < taus.size(); ti++) {
+                const double *row = unav.data() + static_cast<long>(ti) * E + off;
+                for (long k = 0; k < n; k++) put_value(f, row[k]);
+                std::fputc('\n', f);
+            }
+            std::fclose(f);
+        }
+    }
+}
+
+// -A: <prefix>_fft_chunk_<k>-<scale>, one line per (frame, tile) of chunk k with the
+// tile's s*(s/2+1) values of |F/s^2|^2 (calculateAmplitude, src/DDM_kernel.cuh:107-121). The
+// reference names every chunk's file _fft_chunk_<dumps so far> and so keeps only the last
+// chunk's, and its launch grid leaves most of each line zero; here every chunk keeps its
+// own file and every value is written.
+struct PowerWriter {
+    std::vector<FILE *> files;
+    void open(const std::string &prefix, long chunk_index, const std::vector<int> &scales) {
+        close();
+        for (int s : scales)
+            files.push_back(open_out(prefix + "_fft_chunk_" + std::to_string(chunk_index) + "-" + std::to_string(s)));
+    }
+    void frame(const std::vector<float> &pw, const std::vector<int> &scales) {
+        long off = 0;
+        for (size_t si = 0; si < scales.size(); si++) {
+            const int s = scales[si];
+            const int tiles = (scales[0] / s) * (scales[0] / s);
+            const long n = static_cast<long>(s) * (s / 2 + 1);
+            for (int tile = 0; tile < tiles; tile++, off += n) {
+                for (long k = 0; k < n; k++) put_value(files[si], pw[off + k]);
+                std::fputc('\n', files[si]);
+            }
+        }
+    }
+    void close() {
+        for (FILE *f : files) std::fclose(f);
+        files.clear();
+    }
+};
 
 template <typename T>
 std::vector<T> read_values(const std::string &path, const char *what) {
@@ -89,7 +166,7 @@ int main(int argc, char **argv) {
     std::string file_in, file_out, q_file, t_file, s_file;
     int frame_count = 0, frame_offset = 0, x_off = 0, y_off = 0, chunk = 100, rolling = 0;
     bool use_index_fps = false, multistream = true, bench = false, movie = false;
-    bool input_specified = false;
+    bool input_specified = false, unaveraged_out = false, power_out = false;
     float tolerance = 1.2f;
     int estimator = DDM_EST_COMPAT, pixel_mode = DDM_PIX_BYTE0;
 
@@ -122,8 +199,8 @@ int main(int argc, char **argv) {
             case 'M': movie = true; break;
             case 'G': rolling = std::atoi(optarg); break;
             case 'F': break;  // the reference stores the value but never enables it (src/main.cpp:214-219)
-            case 'K':
-            case 'A': die("the -K and -A debug outputs are not produced by this build");
+            case 'K': unaveraged_out = true; break;  // takes an argument, as in the reference
+            case 'A': power_out = true; break;
             case 'E':
                 if (!std::strcmp(optarg, "compat")) estimator = DDM_EST_COMPAT;
                 else if (!std::strcmp(optarg, "unbiased")) estimator = DDM_EST_UNBIASED;
@@ -262,13 +339,35 @@ int main(int argc, char **argv) {
     int dumps_written = 0;
     long sent = 0;
     int which = 0;
+    PowerWriter power;
+    std::vector<float> pw(power_out ? ddm_frame_elements(eng) : 0);
     while (sent < frames_total) {
         const int n = static_cast<int>(std::min<long>(chunk, frames_total - sent));
         if (!bench && ddm_movie_read(mv, buf[which], n) != DDM_OK) {
             std::fprintf(stderr, "%s\n", ddm_last_error());
             return EXIT_FAILURE;
         }
-        if (ddm_submit_frames(eng, buf[which], n, 0) != DDM_OK) die(ddm_last_error());
+        if (!power_out) {
+            if (ddm_submit_frames(eng, buf[which], n, 0) != DDM_OK) die(ddm_last_error());
+        } else {
+            // -A: submit in pieces no larger than the engine's ingest piece (min(C, 32) frames;
+            // the ring holds at least that many latest frames), reading each piece's spectra
+            power.open(file_out, sent / chunk, scales);
+            const int step = std::max(1, std::min({chunk, 32, info.ring_slots}));
+            for (int f0 = 0; f0 < n; f0 += step) {
+                const int m = std::min(step, n - f0);
+                if (ddm_submit_frames(eng, buf[which] + frame_bytes * f0, m, 0) != DDM_OK ||
+                    ddm_synchronize(eng) != DDM_OK)
+                    die(ddm_last_error());
+                for (int f = 0; f < m; f++) {
+                    if (ddm_read_power_spectrum(eng, static_cast<int>(sent + f0 + f), pw.data(),
+                                                static_cast<long>(pw.size())) != DDM_OK)
+                        die(ddm_last_error());
+                    power.frame(pw, scales);
+                }
+            }
+            power.close();
+        }
         sent += n;
         which ^= 1;
         // the other buffer is refilled next: its copy must have finished (benchmark mode
@@ -294,6 +393,12 @@ int main(int argc, char **argv) {
     }
     if (ddm_read_isf(eng, isf.data(), static_cast<long>(isf.size())) != DDM_OK) die(ddm_last_error());
     write_all(file_out);
+    if (unaveraged_out) {
+        const long E = ddm_frame_elements(eng);
+        std::vector<double> unav(static_cast<size_t>(E) * taus.size());
+        if (ddm_read_unaveraged(eng, unav.data(), static_cast<long>(unav.size())) != DDM_OK) die(ddm_last_error());
+        write_unaveraged(file_out, unav, E, scales, lambdas, taus, int_fps);
+    }
     auto t_end = std::chrono::high_resolution_clock::now();
 
     ddm_close(eng);

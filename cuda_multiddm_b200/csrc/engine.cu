@@ -881,6 +881,44 @@ extern "C" int ddm_read_accumulators(ddm_engine *e, double *out, long capacity) 
     return DDM_OK;
 }
 
+extern "C" int ddm_read_power_spectrum(ddm_engine *e, int frame, float *out, long capacity) {
+    clear_error();
+    if (!e || !out || capacity < e->E) return fail(DDM_ERR_INVALID_ARG, "ddm_read_power_spectrum: bad argument");
+    std::vector<float> spec(2 * static_cast<size_t>(e->E));
+    int st = ddm_read_spectrum(e, frame, spec.data(), static_cast<long>(spec.size()));
+    if (st) return st;
+    // src/DDM_kernel.cuh:107-121 (calculateAmplitude): v = F / s^2 in float, then |v|^2
+    for (const ScaleDesc &d : e->sd) {
+        const float fft_norm = 1.0f / static_cast<float>(d.s * d.s);
+        const long long end = d.off + d.tiles * d.n;
+        for (long long k = d.off; k < end; k++) {
+            const float x = fft_norm * spec[2 * k], y = fft_norm * spec[2 * k + 1];
+            out[k] = x * x + y * y;
+        }
+    }
+    return DDM_OK;
+}
+
+extern "C" int ddm_read_unaveraged(ddm_engine *e, double *out, long capacity) {
+    clear_error();
+    if (!e || !out || capacity < static_cast<long>(e->T * e->E))
+        return fail(DDM_ERR_INVALID_ARG, "ddm_read_unaveraged: bad argument");
+    if (!e->finalized) return fail(DDM_ERR_STATE, "ddm_finalize has not run");
+    std::vector<float2> tmp(static_cast<size_t>(e->T) * e->E);
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    CUDA_TRY(cudaMemcpy(tmp.data(), e->acc, sizeof(float2) * tmp.size(), cudaMemcpyDeviceToHost));
+    for (int t = 0; t < e->T; t++) {
+        const double nrm = e->host_norm[t];
+        for (const ScaleDesc &d : e->sd) {
+            const double f = nrm != 0.0 ? 2.0 * d.inv_s4 / nrm : 0.0;
+            const size_t b = static_cast<size_t>(t) * e->E + d.off, n = static_cast<size_t>(d.tiles) * d.n;
+            for (size_t k = b; k < b + n; k++)
+                out[k] = (static_cast<double>(tmp[k].x) - static_cast<double>(tmp[k].y)) * f;
+        }
+    }
+    return DDM_OK;
+}
+
 extern "C" int ddm_get_info(const ddm_engine *e, ddm_info *info) {
     if (!e || !info) return fail(DDM_ERR_INVALID_ARG, "bad argument");
     info->frames_submitted = static_cast<long>(e->submitted);

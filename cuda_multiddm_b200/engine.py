@@ -167,6 +167,19 @@ class Engine:
         check(lib().ddm_read_accumulators(self._h, out.ctypes.data, out.size))
         return out.reshape(len(self.taus), self.frame_elements)
 
+    def power_spectrum(self, frame: int) -> np.ndarray:
+        """|F / s^2|^2 per element of a frame still in the ring (the -A output)."""
+        out = np.zeros(self.frame_elements, np.float32)
+        check(lib().ddm_read_power_spectrum(self._h, frame, out.ctypes.data, out.size))
+        return out
+
+    def unaveraged(self) -> np.ndarray:
+        """[tau, element] structure function before the azimuthal average (the -K output),
+        after finalize()."""
+        out = np.zeros(len(self.taus) * self.frame_elements, np.float64)
+        check(lib().ddm_read_unaveraged(self._h, out.ctypes.data, out.size))
+        return out.reshape(len(self.taus), self.frame_elements)
+
     def set_timing(self, enabled: bool = True) -> None:
         check(lib().ddm_set_timing(self._h, int(enabled)))
 

@@ -144,6 +144,19 @@ long ddm_frame_elements(const ddm_engine *e);
 int ddm_read_spectrum(ddm_engine *e, int frame, float *out, long capacity);
 int ddm_read_accumulators(ddm_engine *e, double *out, long capacity);
 
+/* The -A output (src/DDM.cu:196-211 with calculateAmplitude, src/DDM_kernel.cuh:107-121):
+ * |F / s^2|^2 in float for every element of frame `frame` (still in the ring), layout
+ * [scale][tile][ky][kx]. Unlike the reference, every element is written (its launch grid
+ * covers only part of the array). */
+int ddm_read_power_spectrum(ddm_engine *e, int frame, float *out, long capacity);
+
+/* The -K output, corrected (the reference writes raw accumulator rows with a wrong row
+ * stride, src/azimuthal_average.cu:62-106, from the tile offset of src/DDM.cu:122): after
+ * ddm_finalize, for every tau and element [tau][scale][tile][ky][kx] the value
+ * 2 * sum|dF|^2 / s^4 / norm[tau] with the norms that finalize used, i.e. the
+ * per-wave-vector structure function whose mean over each annulus mask is the ISF bin. */
+int ddm_read_unaveraged(ddm_engine *e, double *out, long capacity);
+
 /* Engine facts: frames submitted, ring slots, device bytes held, kernels launched so far,
  * the stream the engine runs on (a cudaStream_t), and for DDM_EST_COMPAT the number of
  * frames the reference schedule reads (max(N, 2C) when N < 2C, else N; 0 otherwise). */

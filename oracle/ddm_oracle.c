@@ -303,11 +303,14 @@ static void accumulate_pair(double *acc_t, const double *fa, const double *fb, l
     }
 }
 
-int orc_ddm_run(const unsigned char *frames, int nframes, int w, int h, int bpp, int pixmode,
-                int x_off, int y_off, const int *scales, int S, const int *taus, int T,
-                const float *lambdas, int Q, float tolerance, int N, int C, int multistream,
-                int estimator, int G, double *isf, double *dumps, int max_dumps) {
+static int ddm_run_impl(const unsigned char *frames, int nframes, int w, int h, int bpp, int pixmode,
+                        int x_off, int y_off, const int *scales, int S, const int *taus, int T,
+                        const float *lambdas, int Q, float tolerance, int N, int C, int multistream,
+                        int estimator, int G, double *isf, double *dumps, int max_dumps, double *unav) {
     const int M = scales[0];
+    long E_all = 0; /* complex elements per frame over all scales (unaveraged layout) */
+    for (int si = 0; si < S; si++) E_all += (long)(M / scales[si]) * (M / scales[si]) * scales[si] * (scales[si] / 2 + 1);
+    long e_off = 0;
     if (M + x_off > w || M + y_off > h) return -2;
     int ncalls_max = N + C;
     int *A = NULL, *B = NULL, *ep = NULL;
@@ -369,6 +372,12 @@ int orc_ddm_run(const unsigned char *frames, int nframes, int w, int h, int bpp,
         }
         orc_azimuthal(acc, s, tiles, T, lambdas, Q, tolerance, norm, isf + isf_off);
         isf_off += (long)tiles * Q * T;
+        if (unav) { /* 2 * mean |dF|^2 / s^4 per element: its annulus means are the ISF */
+            for (int t = 0; t < T; t++)
+                for (long k = 0; k < fsz; k++)
+                    unav[(long)t * E_all + e_off + k] = norm[t] > 0.0 ? 2.0 * acc[(long)t * fsz + k] / norm[t] : 0.0;
+        }
+        e_off += fsz;
         free(spec);
         free(acc);
     }
@@ -377,6 +386,22 @@ int orc_ddm_run(const unsigned char *frames, int nframes, int w, int h, int bpp,
     free(B);
     free(ep);
     return ndumps < max_dumps ? ndumps : max_dumps;
+}
+
+int orc_ddm_run(const unsigned char *frames, int nframes, int w, int h, int bpp, int pixmode,
+                int x_off, int y_off, const int *scales, int S, const int *taus, int T,
+                const float *lambdas, int Q, float tolerance, int N, int C, int multistream,
+                int estimator, int G, double *isf, double *dumps, int max_dumps) {
+    return ddm_run_impl(frames, nframes, w, h, bpp, pixmode, x_off, y_off, scales, S, taus, T, lambdas, Q,
+                        tolerance, N, C, multistream, estimator, G, isf, dumps, max_dumps, NULL);
+}
+
+int orc_ddm_run_unaveraged(const unsigned char *frames, int nframes, int w, int h, int bpp, int pixmode,
+                           int x_off, int y_off, const int *scales, int S, const int *taus, int T,
+                           const float *lambdas, int Q, float tolerance, int N, int C, int multistream,
+                           int estimator, double *isf, double *unav) {
+    return ddm_run_impl(frames, nframes, w, h, bpp, pixmode, x_off, y_off, scales, S, taus, T, lambdas, Q,
+                        tolerance, N, C, multistream, estimator, 0, isf, NULL, 0, unav);
 }
 
 /* ------------------------------------------------------------------------- */

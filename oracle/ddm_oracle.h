@@ -82,6 +82,17 @@ int orc_ddm_run(const unsigned char *frames, int nframes, int w, int h, int bpp,
                 int total_frames, int chunk, int multistream, int estimator, int dump_every,
                 double *isf, double *dumps, int max_dumps);
 
+/* As orc_ddm_run without -G dumps, also writing the corrected -K output: for every tau and
+ * spectrum element (layout [tau][scale][tile][ky][kx], all scales concatenated),
+ * 2 * sum |dF|^2 / s^4 / norm[tau], the per-wave-vector values whose mean over each annulus
+ * mask is the ISF (the reference writes raw accumulator rows, src/azimuthal_average.cu:62-106,
+ * src/DDM.cu:120-134). */
+int orc_ddm_run_unaveraged(const unsigned char *frames, int nframes, int w, int h, int bpp, int pixmode,
+                           int x_off, int y_off, const int *scales, int scale_count, const int *taus,
+                           int tau_count, const float *lambdas, int lambda_count, float tolerance,
+                           int total_frames, int chunk, int multistream, int estimator, double *isf,
+                           double *unaveraged);
+
 /* Number of doubles in one ISF block: sum over scales of tiles*Q*T. */
 long orc_isf_size(const int *scales, int scale_count, int lambda_count, int tau_count);
 

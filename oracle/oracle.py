@@ -52,6 +52,10 @@ def lib() -> C.CDLL:
         l.orc_ddm_run.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int,
                                   P, C.c_int, P, C.c_int, C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                   P, P, C.c_int]
+        l.orc_ddm_run_unaveraged.restype = C.c_int
+        l.orc_ddm_run_unaveraged.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P,
+                                             C.c_int, P, C.c_int, P, C.c_int, C.c_float, C.c_int, C.c_int, C.c_int,
+                                             C.c_int, P, P]
         l.orc_isf_size.restype = C.c_long
         l.orc_isf_size.argtypes = [P, C.c_int, C.c_int, C.c_int]
         l.orc_azimuthal.restype = None
@@ -158,6 +162,27 @@ def ddm_run_bpp(frames_bytes: np.ndarray, w: int, h: int, bpp: int, scales, taus
     if nd < 0:
         raise RuntimeError(f"orc_ddm_run failed with {nd}")
     return isf, [dumps[i] for i in range(nd)]
+
+
+def ddm_run_unaveraged(frames: np.ndarray, scales, taus, lambdas, *, tol: float = 1.2, chunk: int = 30,
+                       estimator: int = EST_UNBIASED, multistream: bool = True):
+    """uint8 frames [n, h, w] -> (isf, unaveraged [T, E]): the corrected -K output, 2 * mean
+    |dF|^2 / s^4 per spectrum element (all scales concatenated, each [tile][ky][kx])."""
+    fr = np.ascontiguousarray(frames, dtype=np.uint8)
+    n, h, w = fr.shape
+    s = _i32(scales)
+    t = _i32(taus)
+    l = _f32(lambdas)
+    M = int(max(scales))
+    E = sum((M // x) ** 2 * x * (x // 2 + 1) for x in scales)
+    isf = np.zeros(isf_size(s, len(l), len(t)), np.float64)
+    unav = np.zeros((len(t), E), np.float64)
+    st = lib().orc_ddm_run_unaveraged(fr.ctypes.data, n, w, h, 1, PIX_BYTE0, 0, 0, s.ctypes.data, len(s),
+                                      t.ctypes.data, len(t), l.ctypes.data, len(l), C.c_float(tol), n, chunk,
+                                      int(multistream), estimator, isf.ctypes.data, unav.ctypes.data)
+    if st < 0:
+        raise RuntimeError(f"orc_ddm_run_unaveraged failed with {st}")
+    return isf, unav
 
 
 def azimuthal(acc: np.ndarray, scale: int, tiles: int, lambdas, tol: float, norm) -> np.ndarray:

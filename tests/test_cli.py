@@ -105,3 +105,63 @@ def test_cli_benchmark_mode_runs(tmp_path):
                  "-B", "1"])
     assert r.returncode == 0, r.stderr
     assert len(list(tmp_path.glob("b_*"))) == 1 + 4
+
+
+def _read_rows(path):
+    lines = path.read_text().split("\n")
+    assert lines[-1] == ""  # every line ends with a newline
+    return lines[:-1]
+
+
+@pytest.mark.gpu
+def test_cli_debug_outputs_K_and_A(tmp_path):
+    """-K and -A with their corrected contents: -K files hold, per tau, 2 mean|dF|^2 / s^4 of
+    every wave vector (checked against the FP64 oracle, and its annulus means against the ISF
+    file); -A files hold |F/s^2|^2 of every frame and tile of each chunk (against the oracle's
+    FFT)."""
+    from cuda_multiddm_b200.media import synth_video
+    from oracle import oracle as O
+
+    scales, taus, lambdas, C, N = [64, 32], [1, 2, 4], [4.0, 8.0], 10, 30
+    frames = synth_video(61, 64, 64, N, 25, step_var=1.0)
+    movie = tmp_path / "in.movie"
+    write_movie(movie, frames, frame_time_us=1_000_000)
+    ps, pt, pl = write_params(tmp_path, scales, taus, lambdas)
+    out = tmp_path / "out"
+    out.mkdir()
+    r = run_cli(["-o", str(out / "d_"), "-N", str(N), "-C", str(C), "-Q", str(pl), "-T", str(pt), "-S", str(ps),
+                 "-M", "-f", str(movie), "-K", "1", "-A", "-E", "unbiased"])
+    assert r.returncode == 0, r.stderr
+
+    want_isf, want_unav = O.ddm_run_unaveraged(frames, scales, taus, lambdas, chunk=C)
+    off = 0
+    for s in scales:
+        n = s * (s // 2 + 1)
+        m, cnt = O.masks(s, lambdas, 1.2)
+        for tile in range((64 // s) ** 2):
+            rows = _read_rows(out / f"d_{s}-{tile}-nonAve")
+            assert rows[0] == "".join(f"{x:g} " for x in lambdas)
+            assert len(rows) == 2 + len(taus)
+            got = np.array([[float(v) for v in row.split()] for row in rows[2:]])
+            assert got.shape == (len(taus), n)
+            want = want_unav[:, off:off + n]
+            tol = 1e-5 * np.abs(want) + sig_digit_tolerance(want) + 1e-9 * np.abs(want).max()
+            assert np.all(np.abs(got - want) <= tol), (s, tile)
+            isf = parse((out / f"d_{s}-{tile}").read_text())[1]  # [q][tau]
+            for q in range(len(lambdas)):
+                if cnt[q]:
+                    mean = got[:, m[q].reshape(-1).astype(bool)].mean(axis=1)
+                    assert np.allclose(mean, isf[q], rtol=2e-5, atol=1e-9 * np.abs(isf).max())
+            off += n
+
+    for k in range(N // C):
+        for si, s in enumerate(scales):
+            rows = _read_rows(out / f"d__fft_chunk_{k}-{s}")
+            tiles = (64 // s) ** 2
+            assert len(rows) == C * tiles
+            for f in (0, C - 1):
+                tiles_px = O.extract(frames[k * C + f], 1, O.PIX_BYTE0, 0, 0, 64, s)
+                for tile in range(tiles):
+                    want = np.abs(O.fft2_r2c(tiles_px[tile]) / (s * s)).reshape(-1) ** 2
+                    got = np.array([float(v) for v in rows[f * tiles + tile].split()])
+                    assert np.allclose(got, want, rtol=1e-4, atol=1e-6 * want.max())

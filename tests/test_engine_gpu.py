@@ -197,6 +197,32 @@ def test_compat_long_chunk_matches_oracle():
         assert_isf_close(isf, want, scales, len(lambdas), len(taus))
 
 
+def test_unaveraged_and_power_spectrum_match_oracle():
+    """The -K and -A quantities through the C ABI: the per-wave-vector structure function
+    before the azimuthal average (compat and unbiased) and |F / s^2|^2 of a frame."""
+    frames = media.synth_video(47, 128, 128, 40, 60, step_var=1.0)
+    scales, taus, lambdas = [128, 64, 32], [1, 3, 7], [3.0, 6.0, 12.0]
+    for est, oest in (("unbiased", O.EST_UNBIASED), ("compat", O.EST_COMPAT)):
+        cfg = EngineConfig(frame_width=128, frame_height=128, scales=scales, taus=taus, lambdas=lambdas,
+                           chunk_frames=10, estimator=est, total_frames=40)
+        with Engine(cfg) as eng:
+            eng.submit(frames)
+            eng.finalize()
+            got = eng.unaveraged()
+            power = eng.power_spectrum(39)
+        _, want = O.ddm_run_unaveraged(frames, scales, taus, lambdas, chunk=10, estimator=oest)
+        floor = 1e-9 * np.abs(want).max()
+        assert np.all(np.abs(got - want) <= RTOL * np.abs(want) + floor), (est, float(np.abs(got - want).max()))
+    off = 0
+    for s in scales:
+        px = O.extract(frames[39], 1, O.PIX_BYTE0, 0, 0, 128, s)
+        for tile in range(px.shape[0]):
+            want = (np.abs(O.fft2_r2c(px[tile])) / (s * s)).reshape(-1) ** 2
+            n = want.size
+            assert np.allclose(power[off:off + n], want, rtol=1e-5, atol=2e-6 * want.max()), (s, tile)
+            off += n
+
+
 def test_errors_are_status_codes():
     base = dict(frame_width=64, frame_height=64, taus=[1, 2], lambdas=[4.0], chunk_frames=4)
     with pytest.raises(DDMError) as e:

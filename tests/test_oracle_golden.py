@@ -124,3 +124,26 @@ def test_azimuthal_matches_reference_analyse_fft_device(idx):
     for q, t, v in g["isf"]:
         want = out[0, q, t]
         assert abs(want - v) <= 2e-6 * abs(v) + 1e-12, (q, t, want, v)
+
+
+def test_unaveraged_annulus_means_are_the_isf():
+    """The corrected -K quantity (2 mean|dF|^2 / s^4 per wave vector) averages over each
+    annulus mask to the ISF bin: the property that defines the format."""
+    from cuda_multiddm_b200 import media
+
+    frames = media.synth_video(9, 64, 64, 25, 20, step_var=1.0)
+    scales, taus, lambdas = [64, 32], [1, 2, 5], [3.0, 6.0, 12.0]
+    for est in (O.EST_UNBIASED, O.EST_COMPAT):
+        isf, unav = O.ddm_run_unaveraged(frames, scales, taus, lambdas, chunk=10, estimator=est)
+        off = isf_off = 0
+        for s in scales:
+            n = s * (s // 2 + 1)
+            m, cnt = O.masks(s, lambdas, 1.2)
+            for tile in range((64 // s) ** 2):
+                block = isf[isf_off:isf_off + len(lambdas) * len(taus)].reshape(len(lambdas), len(taus))
+                for q in range(len(lambdas)):
+                    if cnt[q]:
+                        mean = unav[:, off:off + n][:, m[q].reshape(-1).astype(bool)].mean(axis=1)
+                        np.testing.assert_allclose(mean, block[q], rtol=1e-12, atol=1e-300)
+                off += n
+                isf_off += len(lambdas) * len(taus)
