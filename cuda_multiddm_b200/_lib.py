@@ -69,6 +69,9 @@ SIGNATURES = {
     "ddm_read_accumulators": (C.c_int, [C.c_void_p, C.c_void_p, C.c_long]),
     "ddm_read_power_spectrum": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_long]),
     "ddm_read_unaveraged": (C.c_int, [C.c_void_p, C.c_void_p, C.c_long]),
+    "ddm_tile_count": (C.c_long, [C.c_void_p]),
+    "ddm_fit_isf": (C.c_int, [C.c_void_p, C.c_float, C.c_double, C.c_int, C.c_void_p, C.c_void_p,
+                              C.c_void_p, C.c_void_p]),
     "ddm_get_info": (C.c_int, [C.c_void_p, C.POINTER(Info)]),
     "ddm_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
     "ddm_kernel_times": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),

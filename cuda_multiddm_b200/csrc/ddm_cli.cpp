@@ -13,6 +13,7 @@
 //   -K ARG -A                               the reference's debug outputs, with corrected
 //                                           contents (see write_unaveraged / write_power)
 // Flags added here:
+//   -D UM_PER_PX         fit the ISF on the GPU (ddm_fit_isf) and write <out>fit
 //   -E compat|unbiased   estimator (default compat: the reference's own pairing)
 //   -P byte0|u16         16-bit pixel decoding (default byte0: the reference's first byte)
 #include <getopt.h>
@@ -72,6 +73,9 @@ void print_help() {
                  "               function of every wave vector before the azimuthal average\n"
                  "  -A           also write <PATH>_fft_chunk_<k>-<scale>: |F/s^2|^2 of every\n"
                  "               frame and tile of chunk k\n"
+                 "  -D UMPX      also fit A(1-exp(-F tau))+B to every ISF curve on the GPU and\n"
+                 "               write <PATH>fit with F, A, B per curve and the diffusion\n"
+                 "               coefficient per tile and scale (UMPX: micrometres per pixel)\n"
                  "  -E MODE      compat (default) or unbiased estimator\n"
                  "  -P MODE      byte0 (default) or u16 decoding of 16-bit pixels\n");
 }
@@ -147,6 +151,41 @@ struct PowerWriter {
     }
 };
 
+// -D: <prefix>fit. Per scale, a line "scale <s> D <D> sigma_D <err>" from the tile-averaged
+// ISF, then per tile "tile <s> <index> D <D> sigma_D <err>", then per (tile, lambda)
+// "curve <s> <index> <lambda> F A B sigma_F sigma_A sigma_B" (tile index -1: tile average).
+void write_fits(const std::string &prefix, ddm_engine *eng, const std::vector<int> &scales,
+                const std::vector<float> &lambdas, float fps, double um_per_px) {
+    const long nt = ddm_tile_count(eng);
+    const size_t S = scales.size(), Q = lambdas.size();
+    std::vector<double> tile_fit(nt * Q * 6), scale_fit(S * Q * 6), tile_d(nt * 2), scale_d(S * 2);
+    if (ddm_fit_isf(eng, fps, um_per_px, DDM_FIT_START_DATA, tile_fit.data(), scale_fit.data(), tile_d.data(),
+                    scale_d.data()) != DDM_OK)
+        die(ddm_last_error());
+    FILE *f = open_out(prefix + "fit");
+    std::fprintf(f, "# I(tau) = A (1 - exp(-F tau)) + B; tau in %s; D in um^2/%s (%g um per px)\n",
+                 fps > 0 ? "s" : "frames", fps > 0 ? "s" : "frame", um_per_px);
+    for (size_t si = 0; si < S; si++)
+        std::fprintf(f, "scale %d D %.9g sigma_D %.9g\n", scales[si], scale_d[2 * si], scale_d[2 * si + 1]);
+    long row = 0;
+    for (size_t si = 0; si < S; si++) {
+        const int tiles = (scales[0] / scales[si]) * (scales[0] / scales[si]);
+        for (int t = 0; t < tiles; t++, row++)
+            std::fprintf(f, "tile %d %d D %.9g sigma_D %.9g\n", scales[si], t, tile_d[2 * row], tile_d[2 * row + 1]);
+    }
+    auto curve = [&](int s, int t, float lam, const double *p) {
+        std::fprintf(f, "curve %d %d %g %.9g %.9g %.9g %.9g %.9g %.9g\n", s, t, lam, p[0], p[1], p[2], p[3], p[4], p[5]);
+    };
+    row = 0;
+    for (size_t si = 0; si < S; si++) {
+        for (size_t q = 0; q < Q; q++) curve(scales[si], -1, lambdas[q], scale_fit.data() + (si * Q + q) * 6);
+        const int tiles = (scales[0] / scales[si]) * (scales[0] / scales[si]);
+        for (int t = 0; t < tiles; t++, row++)
+            for (size_t q = 0; q < Q; q++) curve(scales[si], t, lambdas[q], tile_fit.data() + (row * Q + q) * 6);
+    }
+    std::fclose(f);
+}
+
 template <typename T>
 std::vector<T> read_values(const std::string &path, const char *what) {
     std::ifstream in(path);
@@ -167,11 +206,12 @@ int main(int argc, char **argv) {
     int frame_count = 0, frame_offset = 0, x_off = 0, y_off = 0, chunk = 100, rolling = 0;
     bool use_index_fps = false, multistream = true, bench = false, movie = false;
     bool input_specified = false, unaveraged_out = false, power_out = false;
+    double fit_um_per_px = 0.0;  // -D
     float tolerance = 1.2f;
     int estimator = DDM_EST_COMPAT, pixel_mode = DDM_PIX_BYTE0;
 
     for (;;) {
-        int c = getopt(argc, argv, "ho:N:s:x:y:Q:T:S:If:W::vZt:C:MG:F:B:K:AE:P:");
+        int c = getopt(argc, argv, "ho:N:s:x:y:Q:T:S:If:W::vZt:C:MG:F:B:K:AE:P:D:");
         if (c == -1) break;
         switch (c) {
             case '?':
@@ -201,6 +241,10 @@ int main(int argc, char **argv) {
             case 'F': break;  // the reference stores the value but never enables it (src/main.cpp:214-219)
             case 'K': unaveraged_out = true; break;  // takes an argument, as in the reference
             case 'A': power_out = true; break;
+            case 'D':
+                fit_um_per_px = std::atof(optarg);
+                if (!(fit_um_per_px > 0.0)) die("-D takes the micrometres per pixel (> 0)");
+                break;
             case 'E':
                 if (!std::strcmp(optarg, "compat")) estimator = DDM_EST_COMPAT;
                 else if (!std::strcmp(optarg, "unbiased")) estimator = DDM_EST_UNBIASED;
@@ -399,6 +443,7 @@ int main(int argc, char **argv) {
         if (ddm_read_unaveraged(eng, unav.data(), static_cast<long>(unav.size())) != DDM_OK) die(ddm_last_error());
         write_unaveraged(file_out, unav, E, scales, lambdas, taus, int_fps);
     }
+    if (fit_um_per_px > 0.0) write_fits(file_out, eng, scales, lambdas, int_fps, fit_um_per_px);
     auto t_end = std::chrono::high_resolution_clock::now();
 
     ddm_close(eng);

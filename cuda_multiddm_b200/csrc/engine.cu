@@ -23,6 +23,7 @@
 #include "errors.hpp"
 #include "host.hpp"
 #include "fft.cuh"
+#include "fit.cuh"
 #include "kernels.cuh"
 #include "lag.cuh"
 #include "lag_host.hpp"
@@ -99,6 +100,7 @@ struct ddm_engine {
     double *partial_d = nullptr;                                 // stage-1 azimuthal sums
     long long az_items = 0;
     double *norm_d = nullptr, *isf_d = nullptr;
+    double *fit_d = nullptr;                // ISF fitting: means, tau, q, curve fits, D (first fit call)
     int *status_d = nullptr;                // set by kernels whose bounded waits ran out
     LagMaps maps;                           // 2-D tensor maps of the ring for the lag kernel
     size_t device_bytes = 0;
@@ -166,6 +168,7 @@ void free_all(ddm_engine *e) {
     cudaFree(e->counts_d);
     cudaFree(e->norm_d);
     cudaFree(e->isf_d);
+    cudaFree(e->fit_d);
     cudaFree(e->status_d);
     if (e->tables_h) cudaFreeHost(e->tables_h);
     for (int i = 0; i < kTables; i++)
@@ -916,6 +919,78 @@ extern "C" int ddm_read_unaveraged(ddm_engine *e, double *out, long capacity) {
                 out[k] = (static_cast<double>(tmp[k].x) - static_cast<double>(tmp[k].y)) * f;
         }
     }
+    return DDM_OK;
+}
+
+extern "C" long ddm_tile_count(const ddm_engine *e) {
+    if (!e) return 0;
+    long n = 0;
+    for (const ScaleDesc &d : e->sd) n += d.tiles;
+    return n;
+}
+
+extern "C" int ddm_fit_isf(ddm_engine *e, float fps, double um_per_px, int start, double *tile_fit,
+                           double *scale_fit, double *tile_d, double *scale_d) {
+    clear_error();
+    if (!e) return fail(DDM_ERR_INVALID_ARG, "ddm_fit_isf: null engine");
+    if (!e->finalized) return fail(DDM_ERR_STATE, "ddm_finalize has not run");
+    if (!(um_per_px > 0.0) || !std::isfinite(um_per_px) || !std::isfinite(fps))
+        return fail(DDM_ERR_INVALID_ARG, "ddm_fit_isf: um_per_px must be positive and fps finite");
+    if (start != DDM_FIT_START_DATA && start != DDM_FIT_START_SCRIPT)
+        return fail(DDM_ERR_INVALID_ARG, "ddm_fit_isf: unknown start");
+    const int tiles_total = static_cast<int>(ddm_tile_count(e));
+    const long tile_curves = static_cast<long>(tiles_total) * e->Q, scale_curves = static_cast<long>(e->S) * e->Q;
+    // device layout: mean [S][Q][T], tau [T], q [Q], tile fits, scale fits, tile D, scale D
+    const size_t n_mean = static_cast<size_t>(scale_curves) * e->T;
+    const size_t n_all = n_mean + e->T + e->Q + (tile_curves + scale_curves) * kFitParams + 2 * (tiles_total + e->S);
+    if (!e->fit_d) {
+        int st = dev_alloc(e, &e->fit_d, n_all);
+        if (st) return st;
+    }
+    FitArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.S = e->S, a.T = e->T, a.Q = e->Q;
+    a.start = start == DDM_FIT_START_SCRIPT ? 1 : 0;
+    int curve = 0;
+    for (int si = 0; si < e->S; si++) {
+        a.tiles[si] = e->sd[si].tiles;
+        a.isf_off[si] = e->sd[si].isf_off;
+        a.curve_off[si] = curve;
+        curve += e->sd[si].tiles * e->Q;
+    }
+    a.tile_curves = static_cast<int>(tile_curves);
+    a.isf = e->isf_d;
+    a.mean = e->fit_d;
+    double *tau_d = a.mean + n_mean, *q_d = tau_d + e->T;
+    a.tau = tau_d, a.q = q_d;
+    a.tile_fit = q_d + e->Q;
+    a.scale_fit = a.tile_fit + tile_curves * kFitParams;
+    a.tile_d = a.scale_fit + scale_curves * kFitParams;
+    a.scale_d = a.tile_d + 2 * tiles_total;
+    // lag times as the ISF files label them ((float)tau / fps, src/azimuthal_average.cu:131),
+    // in frames when fps <= 0; q = 2 pi / (lambda * um_per_px) (plot_averaged.py:258-261)
+    std::vector<double> host(static_cast<size_t>(e->T) + e->Q);
+    for (int t = 0; t < e->T; t++)
+        host[t] = fps > 0.0f ? static_cast<double>(static_cast<float>(e->taus[t]) / fps) : e->taus[t];
+    const double two_pi = 6.283185307179586;
+    for (int q = 0; q < e->Q; q++) host[e->T + q] = two_pi / (static_cast<double>(e->lambdas[q]) * um_per_px);
+    CUDA_TRY(cudaMemcpyAsync(tau_d, host.data(), sizeof(double) * host.size(), cudaMemcpyHostToDevice, e->stream));
+    fit_mean_kernel<<<static_cast<unsigned>((n_mean + kFitThreads - 1) / kFitThreads), kFitThreads, 0, e->stream>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    fit_isf_kernel<<<static_cast<unsigned>((tile_curves + scale_curves + kFitThreads - 1) / kFitThreads), kFitThreads,
+                     0, e->stream>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    fit_diffusion_kernel<<<static_cast<unsigned>((tiles_total + e->S + kFitThreads - 1) / kFitThreads), kFitThreads, 0,
+                           e->stream>>>(a, tiles_total);
+    CUDA_TRY(cudaGetLastError());
+    e->launches += 3;
+    CUDA_TRY(cudaStreamSynchronize(e->stream));  // host is a local buffer the copy read from
+    if (tile_fit)
+        CUDA_TRY(cudaMemcpy(tile_fit, a.tile_fit, sizeof(double) * tile_curves * kFitParams, cudaMemcpyDeviceToHost));
+    if (scale_fit)
+        CUDA_TRY(cudaMemcpy(scale_fit, a.scale_fit, sizeof(double) * scale_curves * kFitParams, cudaMemcpyDeviceToHost));
+    if (tile_d) CUDA_TRY(cudaMemcpy(tile_d, a.tile_d, sizeof(double) * 2 * tiles_total, cudaMemcpyDeviceToHost));
+    if (scale_d) CUDA_TRY(cudaMemcpy(scale_d, a.scale_d, sizeof(double) * 2 * e->S, cudaMemcpyDeviceToHost));
     return DDM_OK;
 }
 

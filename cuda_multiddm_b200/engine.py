@@ -180,6 +180,19 @@ class Engine:
         check(lib().ddm_read_unaveraged(self._h, out.ctypes.data, out.size))
         return out.reshape(len(self.taus), self.frame_elements)
 
+    def fit(self, fps: float = 0.0, um_per_px: float = 1.0, start: str = "data") -> dict:
+        """ISF fits after finalize(): {"tile": [tiles, lambda, 6], "scale": [scales, lambda, 6]
+        with (F, A, B, sigma_F, sigma_A, sigma_B), "tile_D": [tiles, 2], "scale_D": [scales, 2]
+        with (D, sigma_D)}. Lag times in seconds (tau / fps) or frames (fps <= 0). start: "data"
+        (read off each curve) or "script" (the reference script's fixed p0)."""
+        nt, S, Q = int(lib().ddm_tile_count(self._h)), len(self.scales), len(self.lambdas)
+        tile, scale = np.zeros((nt, Q, 6)), np.zeros((S, Q, 6))
+        tile_d, scale_d = np.zeros((nt, 2)), np.zeros((S, 2))
+        st = {"data": 0, "script": 1}[start]
+        check(lib().ddm_fit_isf(self._h, C.c_float(fps), C.c_double(um_per_px), st, tile.ctypes.data,
+                                scale.ctypes.data, tile_d.ctypes.data, scale_d.ctypes.data))
+        return {"tile": tile, "scale": scale, "tile_D": tile_d, "scale_D": scale_d}
+
     def set_timing(self, enabled: bool = True) -> None:
         check(lib().ddm_set_timing(self._h, int(enabled)))
 

@@ -157,6 +157,32 @@ int ddm_read_power_spectrum(ddm_engine *e, int frame, float *out, long capacity)
  * per-wave-vector structure function whose mean over each annulus mask is the ISF bin. */
 int ddm_read_unaveraged(ddm_engine *e, double *out, long capacity);
 
+/* Tiles over all scales (sum of (M/s)^2): the row count of ddm_fit_isf's per-tile outputs. */
+long ddm_tile_count(const ddm_engine *e);
+
+/* Starting point of the ISF fits: read off each curve (B = first value, A = largest rise,
+ * F = ln 2 / first lag reaching half of it), or the script's fixed (F, A, B) =
+ * (6, 0.03, 0.004) (plot_averaged.py:77), which suits lags in seconds and F of a few per
+ * second only. */
+typedef enum { DDM_FIT_START_DATA = 0, DDM_FIT_START_SCRIPT = 1 } ddm_fit_start;
+
+/* Fits the ISF of the last ddm_finalize on the GPU, the analysis of the reference's
+ * resources/python_tools/plot_averaged.py:57-141 (run there with scipy on ISF files):
+ * I(tau) = A (1 - exp(-F tau)) + B per (scale, tile, lambda) curve and per (scale, lambda)
+ * curve of the tile-averaged ISF, by FP64 Levenberg-Marquardt from `start`
+ * (ddm_fit_start), with 1-sigma errors as scipy's curve_fit reports them
+ * (covariance (J^T J)^-1 * RSS / (T - 3)); then the diffusion coefficient from
+ * ln F = ln D + 2 ln q (slope fixed at 2) over the lambdas with F > 0, q = 2 pi /
+ * (lambda * um_per_px), per tile and per scale. Lag times are (float)tau / fps as the ISF
+ * files label them, or frames when fps <= 0; D is then in um^2 per second (or per frame).
+ * Outputs (each may be NULL): tile_fit [tiles][lambda][6] and scale_fit [scale][lambda][6]
+ * hold F, A, B, sigma_F, sigma_A, sigma_B; tile_d [tiles][2] and scale_d [scale][2] hold D,
+ * sigma_D (NaN where no lambda gave F > 0). Tiles run over scales (descending), then tile
+ * index. The script itself fits the last tile's ISF where it means the average
+ * (plot_averaged.py:280 passes the loop variable ISF, not ISF_scale); both are here. */
+int ddm_fit_isf(ddm_engine *e, float fps, double um_per_px, int start, double *tile_fit, double *scale_fit,
+                double *tile_d, double *scale_d);
+
 /* Engine facts: frames submitted, ring slots, device bytes held, kernels launched so far,
  * the stream the engine runs on (a cudaStream_t), and for DDM_EST_COMPAT the number of
  * frames the reference schedule reads (max(N, 2C) when N < 2C, else N; 0 otherwise). */

@@ -130,8 +130,16 @@ def test_cli_debug_outputs_K_and_A(tmp_path):
     out = tmp_path / "out"
     out.mkdir()
     r = run_cli(["-o", str(out / "d_"), "-N", str(N), "-C", str(C), "-Q", str(pl), "-T", str(pt), "-S", str(ps),
-                 "-M", "-f", str(movie), "-K", "1", "-A", "-E", "unbiased"])
+                 "-M", "-f", str(movie), "-K", "1", "-A", "-E", "unbiased", "-D", "0.5"])
     assert r.returncode == 0, r.stderr
+
+    # -D: the fit file's layout (values are checked against scipy in test_fit.py)
+    fit = (out / "d_fit").read_text().splitlines()
+    assert fit[0].startswith("# I(tau) = A (1 - exp(-F tau)) + B; tau in s")
+    kinds = [ln.split()[0] for ln in fit[1:]]
+    assert kinds.count("scale") == 2 and kinds.count("tile") == 1 + 4
+    assert kinds.count("curve") == (2 + 1 + 4) * len(lambdas)
+    assert all(np.isfinite(float(ln.split()[5])) for ln in fit[1:] if ln.startswith("curve"))
 
     want_isf, want_unav = O.ddm_run_unaveraged(frames, scales, taus, lambdas, chunk=C)
     off = 0
