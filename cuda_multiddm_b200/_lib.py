@@ -13,7 +13,7 @@ LIB_PATH = PKG / "libddm_b200.so"
 
 DDM_OK = 0
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of device memory", 4: "invalid state",
-          5: "frames missing", 6: "no suitable CUDA device", 7: "I/O error"}
+          5: "frames missing", 6: "no suitable CUDA device", 7: "I/O error", 8: "busy"}
 
 PIX_BYTE0, PIX_U16LE = 0, 1
 EST_COMPAT, EST_UNBIASED = 0, 1
@@ -44,6 +44,20 @@ class Info(C.Structure):
                 ("kernel_launches", C.c_long), ("stream", C.c_void_p), ("frames_needed", C.c_long)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int), ("hbm_budget_bytes", C.c_size_t), ("max_streams", C.c_int),
+                ("results_per_stream", C.c_int)]
+
+
+class ChunkResult(C.Structure):
+    _fields_ = [("chunk_index", C.c_long), ("frames", C.c_long), ("submit_s", C.c_double), ("done_s", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("streams", C.c_int), ("device_bytes", C.c_size_t), ("budget_bytes", C.c_size_t),
+                ("batched_launches", C.c_long), ("chunks_pending", C.c_long)]
+
+
 class MovieInfo(C.Structure):
     _fields_ = [("width", C.c_int), ("height", C.c_int), ("bytes_per_pixel", C.c_int), ("fps", C.c_float),
                 ("camera_type", C.c_int), ("pixel_mode", C.c_int)]
@@ -70,6 +84,16 @@ SIGNATURES = {
     "ddm_read_power_spectrum": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_long]),
     "ddm_read_unaveraged": (C.c_int, [C.c_void_p, C.c_void_p, C.c_long]),
     "ddm_tile_count": (C.c_long, [C.c_void_p]),
+    "ddm_server_open": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]),
+    "ddm_server_close": (C.c_int, [C.c_void_p]),
+    "ddm_server_add_stream": (C.c_int, [C.c_void_p, C.POINTER(Config), C.POINTER(C.c_int)]),
+    "ddm_server_remove_stream": (C.c_int, [C.c_void_p, C.c_int]),
+    "ddm_server_submit": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
+    "ddm_server_step": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "ddm_server_poll": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(ChunkResult), C.c_void_p, C.c_long]),
+    "ddm_server_wait": (C.c_int, [C.c_void_p]),
+    "ddm_server_clock": (C.c_double, [C.c_void_p]),
+    "ddm_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
     "ddm_fit_isf": (C.c_int, [C.c_void_p, C.c_float, C.c_double, C.c_int, C.c_void_p, C.c_void_p,
                               C.c_void_p, C.c_void_p]),
     "ddm_get_info": (C.c_int, [C.c_void_p, C.POINTER(Info)]),

@@ -26,6 +26,7 @@
 #include "fit.cuh"
 #include "kernels.cuh"
 #include "lag.cuh"
+#include "engine_internal.hpp"
 #include "lag_host.hpp"
 
 namespace ddm {
@@ -100,9 +101,13 @@ struct ddm_engine {
     double *partial_d = nullptr;                                 // stage-1 azimuthal sums
     long long az_items = 0;
     double *norm_d = nullptr, *isf_d = nullptr;
+    double *norm_h = nullptr;               // pinned source of the norm upload
+    cudaEvent_t norm_ev = nullptr;          // that upload has read norm_h
     double *fit_d = nullptr;                // ISF fitting: means, tau, q, curve fits, D (first fit call)
     int *status_d = nullptr;                // set by kernels whose bounded waits ran out
     LagMaps maps;                           // 2-D tensor maps of the ring for the lag kernel
+    bool defer_lag = false;                 // served: lag launches are collected, not issued
+    std::vector<DeferredLag> deferred;
     size_t device_bytes = 0;
     std::vector<int> counts_h;             // [S][Q]
     std::vector<std::vector<int>> q_ptr_s, idx_s;  // per scale CSR (host copy)
@@ -169,6 +174,8 @@ void free_all(ddm_engine *e) {
     cudaFree(e->norm_d);
     cudaFree(e->isf_d);
     cudaFree(e->fit_d);
+    if (e->norm_h) cudaFreeHost(e->norm_h);
+    if (e->norm_ev) cudaEventDestroy(e->norm_ev);
     cudaFree(e->status_d);
     if (e->tables_h) cudaFreeHost(e->tables_h);
     for (int i = 0; i < kTables; i++)
@@ -300,6 +307,10 @@ int launch_lag(ddm_engine *e, const Launch &L) {
 
     const unsigned blocks = static_cast<unsigned>((e->E + lag_cta_elems(J) - 1) / lag_cta_elems(J));
     const size_t smem = lag_smem_bytes(J, ntab);
+    if (e->defer_lag) {  // a server issues it with other engines' work in one launch
+        e->deferred.push_back(DeferredLag{J, td, blocks, smem});
+        return DDM_OK;
+    }
     TimedRange tr(e, 1);
     switch (J) {
 #define LAG_CASE(JJ)                                                                                   \
@@ -388,9 +399,11 @@ int lag_iteration(ddm_engine *e, const CompatIteration &it) {
 }
 
 int run_azimuth(ddm_engine *e, const std::vector<double> &norm) {
-    CUDA_TRY(cudaMemcpyAsync(e->norm_d, norm.data(), sizeof(double) * e->T, cudaMemcpyHostToDevice,
-                             e->stream));
-    // the copy reads host memory asynchronously: keep the source alive until it ran
+    // the upload reads norm_h asynchronously: refill it only once the previous one has run
+    CUDA_TRY(cudaEventSynchronize(e->norm_ev));
+    std::copy(norm.begin(), norm.end(), e->norm_h);
+    CUDA_TRY(cudaMemcpyAsync(e->norm_d, e->norm_h, sizeof(double) * e->T, cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(cudaEventRecord(e->norm_ev, e->stream));
     e->host_norm = norm;
     AzArgs a;
     std::memset(&a, 0, sizeof(a));
@@ -436,6 +449,7 @@ int snapshot(ddm_engine *e, const std::vector<double> &norm) {
     int st = run_azimuth(e, norm);
     if (st) return st;
     std::vector<double> out(e->isf_size);
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
     CUDA_TRY(cudaMemcpy(out.data(), e->isf_d, sizeof(double) * e->isf_size, cudaMemcpyDeviceToHost));
     e->dumps.push_back(std::move(out));
     return purge(e);
@@ -625,6 +639,9 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
     if ((st = dev_alloc(e, &e->isf_d, e->isf_size))) return bail(st);
     if ((st = dev_alloc(e, &e->status_d, 1))) return bail(st);
     if (cudaMemset(e->status_d, 0, sizeof(int)) != cudaSuccess) return bail(fail(DDM_ERR_CUDA, "status memset failed"));
+    if (cudaMallocHost(reinterpret_cast<void **>(&e->norm_h), sizeof(double) * e->T) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e->norm_ev, cudaEventDisableTiming) != cudaSuccess)
+        return bail(fail(DDM_ERR_OUT_OF_MEMORY, "pinned norm buffer"));
     if (cudaMallocHost(reinterpret_cast<void **>(&e->tables_h),
                        sizeof(int) * static_cast<size_t>(kTables) * e->tab_stride) != cudaSuccess)
         return bail(fail(DDM_ERR_OUT_OF_MEMORY, "pinned table buffer"));
@@ -775,9 +792,9 @@ extern "C" int ddm_submit_frames(ddm_engine *e, const void *frames, int count, i
     return DDM_OK;
 }
 
-extern "C" int ddm_finalize(ddm_engine *e) {
-    clear_error();
-    if (!e) return fail(DDM_ERR_INVALID_ARG, "ddm_finalize: null engine");
+namespace ddm {
+
+int engine_finalize_async(ddm_engine *e) {
     int st;
     std::vector<double> norm(e->T);
     if (e->estimator == DDM_EST_COMPAT) {
@@ -789,9 +806,32 @@ extern "C" int ddm_finalize(ddm_engine *e) {
         norm = e->pair_count;
     }
     if ((st = run_azimuth(e, norm))) return st;
-    if ((st = check_device_status(e))) return st;
     e->finalized = true;
     return DDM_OK;
+}
+
+void engine_defer_lag(ddm_engine *e, bool on) { e->defer_lag = on; }
+
+std::vector<DeferredLag> engine_take_deferred(ddm_engine *e) {
+    std::vector<DeferredLag> out;
+    out.swap(e->deferred);
+    return out;
+}
+
+LagTarget engine_lag_target(const ddm_engine *e) { return LagTarget{e->ring, e->acc, e->E, e->status_d, &e->maps}; }
+
+cudaStream_t engine_stream(const ddm_engine *e) { return e->stream; }
+const double *engine_isf_device(const ddm_engine *e) { return e->isf_d; }
+const int *engine_status_device(const ddm_engine *e) { return e->status_d; }
+
+}  // namespace ddm
+
+extern "C" int ddm_finalize(ddm_engine *e) {
+    clear_error();
+    if (!e) return fail(DDM_ERR_INVALID_ARG, "ddm_finalize: null engine");
+    int st = engine_finalize_async(e);
+    if (st) return st;
+    return check_device_status(e);
 }
 
 extern "C" long ddm_isf_size(const ddm_engine *e) { return e ? static_cast<long>(e->isf_size) : 0; }
@@ -1102,6 +1142,7 @@ extern "C" const char *ddm_status_string(int status) {
         case DDM_ERR_NEED_FRAMES: return "frames missing";
         case DDM_ERR_NO_DEVICE: return "no suitable CUDA device";
         case DDM_ERR_IO: return "I/O error";
+        case DDM_ERR_BUSY: return "busy";
         default: return "unknown status";
     }
 }

@@ -161,11 +161,12 @@ struct LagMaps {
 // kGS = lag_group_slots(J); its consecutive ring slots arrive as a few 2-D boxes (runs) that
 // all complete on full[g % kGS]; empty[g % kGS] completes when every consumer warp has moved
 // past the group. Union entry u therefore sits in shared-memory slot u % lag_ring_slots(J).
-// Neither side ever waits for the whole CTA.
+// Neither side ever waits for the whole CTA. `block` is the CTA's element block; `maps` may
+// live in kernel parameter space or global memory.
 template <int J>
-__global__ void __launch_bounds__(kLagThreads, 3)
-    lag_pipe_kernel(const float2 *__restrict__ ring, float2 *__restrict__ acc, long long E,
-                    const int *__restrict__ table, int *__restrict__ status, const __grid_constant__ LagMaps maps) {
+__device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, float2 *__restrict__ acc, long long E,
+                                              const int *__restrict__ table, int *__restrict__ status,
+                                              const LagMaps &maps, int block) {
     constexpr int kLanes = lag_lanes(J);
     constexpr int kJT = J / kLanes;  // register frames per thread
     constexpr int kElems = lag_cta_elems(J);
@@ -204,7 +205,7 @@ __global__ void __launch_bounds__(kLagThreads, 3)
     const int *uslot = ent_full + ntau;
     const int *gptr = uslot + nu;
     const int *runs = gptr + ngroups + 1;
-    const long long e0 = static_cast<long long>(blockIdx.x) * kElems;
+    const long long e0 = static_cast<long long>(block) * kElems;
 
     if (warp == kLagConsumerWarps) {
         // ---------------- producer: group g is fill g / kGS of group slot g % kGS
@@ -336,6 +337,41 @@ __global__ void __launch_bounds__(kLagThreads, 3)
         }
         __syncthreads();
     }
+}
+
+// One engine's launch: CTA b handles element block b.
+template <int J>
+__global__ void __launch_bounds__(kLagThreads, 3)
+    lag_pipe_kernel(const float2 *__restrict__ ring, float2 *__restrict__ acc, long long E,
+                    const int *__restrict__ table, int *__restrict__ status, const __grid_constant__ LagMaps maps) {
+    lag_pipe_body<J>(ring, acc, E, table, status, maps, static_cast<int>(blockIdx.x));
+}
+
+// The lag work of several engines (served streams) in one launch: item i owns CTAs
+// [cta_begin, next item's cta_begin) and runs its own ring, accumulators, table and tensor
+// maps (64-byte aligned, in global memory) exactly as its own launch would.
+struct LagBatchItem {
+    const float2 *ring;
+    float2 *acc;
+    long long E;
+    const int *table;
+    int *status;
+    const LagMaps *maps;
+    int cta_begin;
+    int pad;
+};
+
+template <int J>
+__global__ void __launch_bounds__(kLagThreads, 3)
+    lag_batch_kernel(const LagBatchItem *__restrict__ items, int n) {
+    int lo = 0, hi = n - 1;  // the last item whose first CTA is at or before this one
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (items[mid].cta_begin <= static_cast<int>(blockIdx.x)) lo = mid;
+        else hi = mid - 1;
+    }
+    const LagBatchItem &it = items[lo];
+    lag_pipe_body<J>(it.ring, it.acc, it.E, it.table, it.status, *it.maps, static_cast<int>(blockIdx.x) - it.cta_begin);
 }
 
 // Dynamic shared memory of a launch of lag_pipe_kernel<J> with a table of table_ints ints

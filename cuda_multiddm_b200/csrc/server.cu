@@ -1,0 +1,409 @@
+// Serving many DDM streams on one GPU: admission by HBM footprint, per-stream device state
+// (FFT ring, accumulators) kept resident, and continuous batching: every step takes the
+// next pending chunk of every stream that has one, runs each stream's FFT, then ONE lag
+// launch (per register-frame count) over all those streams' lag work, then each stream's
+// azimuthal average and the copy of its ISF to host memory. Steps do not wait for the GPU:
+// a stream's result is ready when a host callback queued behind its copy has run, so
+// chunks that arrive while earlier ones are on the GPU are taken by the next step.
+// (The reference analyses one video per process: src/DDM.cu:268-892.)
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/ddm.h"
+#include "engine_internal.hpp"
+#include "errors.hpp"
+#include "lag.cuh"
+
+using namespace ddm;
+
+namespace {
+
+constexpr int kItemRing = 4;  // batch descriptor buffers in flight
+
+using Clock = std::chrono::steady_clock;
+
+struct PinnedBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+struct Slot {  // one chunk on its way through the GPU, and its result
+    double *isf_h = nullptr;  // pinned
+    int *status_h = nullptr;  // pinned
+    PinnedBuf frames;         // the chunk's frames (held until the result is in)
+    long chunk_index = 0;
+    long frames_done = 0;
+    double submit_s = 0.0;
+    std::atomic<double> done_s{0.0};
+    std::atomic<int> state{0};  // 0 free, 1 on the GPU, 2 result ready
+    const ddm_server *server = nullptr;
+};
+
+struct PendingChunk {
+    PinnedBuf frames;
+    int count;
+    double submit_s;
+};
+
+struct Stream {
+    ddm_engine *eng = nullptr;
+    size_t bytes = 0;
+    size_t frame_bytes = 0;
+    long isf_size = 0;
+    long chunks_submitted = 0, chunks_issued = 0, frames_issued = 0;
+    LagMaps *maps_d = nullptr;
+    std::deque<PendingChunk> pending;
+    std::vector<std::unique_ptr<Slot>> slots;
+    std::deque<Slot *> order;  // slots in flight or ready, in chunk order
+    std::vector<PinnedBuf> free_bufs;
+};
+
+void CUDART_CB on_result(void *arg) {  // runs on a CUDA driver thread: no CUDA calls here
+    Slot *s = static_cast<Slot *>(arg);
+    s->done_s.store(ddm_server_clock(s->server));
+    s->state.store(2);
+}
+
+}  // namespace
+
+struct ddm_server {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    size_t budget = 0, used = 0;
+    int max_streams = 64, results_per_stream = 4;
+    Clock::time_point t0 = Clock::now();
+    int next_id = 1;
+    std::map<int, Stream> streams;
+    mutable std::mutex lock;
+    // batched lag descriptors
+    LagBatchItem *items_h = nullptr, *items_d = nullptr;
+    int items_cap = 0, items_next = 0;
+    cudaEvent_t items_ev[kItemRing] = {};
+    bool items_used[kItemRing] = {};
+    long launches = 0;
+};
+
+namespace {
+
+#define CUDA_TRY(expr)                                                                            \
+    do {                                                                                          \
+        cudaError_t err__ = (expr);                                                               \
+        if (err__ != cudaSuccess) return fail(DDM_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(err__)); \
+    } while (0)
+
+int pinned(PinnedBuf *b, size_t bytes) {
+    if (b->bytes >= bytes) return DDM_OK;
+    if (b->p) cudaFreeHost(b->p);
+    b->p = nullptr;
+    b->bytes = 0;
+    if (cudaMallocHost(&b->p, bytes) != cudaSuccess) return fail(DDM_ERR_OUT_OF_MEMORY, "pinned host buffer");
+    b->bytes = bytes;
+    return DDM_OK;
+}
+
+void release_stream(Stream &st) {
+    if (st.eng) ddm_close(st.eng);
+    cudaFree(st.maps_d);
+    for (auto &sl : st.slots) {
+        if (sl->isf_h) cudaFreeHost(sl->isf_h);
+        if (sl->status_h) cudaFreeHost(sl->status_h);
+        if (sl->frames.p) cudaFreeHost(sl->frames.p);
+    }
+    for (auto &pc : st.pending)
+        if (pc.frames.p) cudaFreeHost(pc.frames.p);
+    for (auto &b : st.free_bufs)
+        if (b.p) cudaFreeHost(b.p);
+    st = Stream();
+}
+
+int ensure_items(ddm_server *s, int n) {
+    if (n <= s->items_cap) return DDM_OK;
+    CUDA_TRY(cudaStreamSynchronize(s->stream));  // no batch descriptors in flight
+    if (s->items_h) cudaFreeHost(s->items_h);
+    cudaFree(s->items_d);
+    s->items_h = nullptr;
+    s->items_d = nullptr;
+    const int cap = std::max(n, 64);
+    if (cudaMallocHost(reinterpret_cast<void **>(&s->items_h), sizeof(LagBatchItem) * cap * kItemRing) != cudaSuccess ||
+        cudaMalloc(reinterpret_cast<void **>(&s->items_d), sizeof(LagBatchItem) * cap * kItemRing) != cudaSuccess)
+        return fail(DDM_ERR_OUT_OF_MEMORY, "batch descriptor buffers");
+    s->items_cap = cap;
+    std::fill(s->items_used, s->items_used + kItemRing, false);
+    return DDM_OK;
+}
+
+// One launch of lag_batch_kernel<J> over `work` (engine, its deferred launches of this J).
+int launch_batch(ddm_server *s, int J, const std::vector<std::pair<Stream *, DeferredLag>> &work) {
+    if (work.empty()) return DDM_OK;
+    int st = ensure_items(s, static_cast<int>(work.size()));
+    if (st) return st;
+    const int ring = s->items_next;
+    s->items_next = (s->items_next + 1) % kItemRing;
+    if (s->items_used[ring]) CUDA_TRY(cudaEventSynchronize(s->items_ev[ring]));
+    LagBatchItem *h = s->items_h + static_cast<size_t>(ring) * s->items_cap;
+    LagBatchItem *d = s->items_d + static_cast<size_t>(ring) * s->items_cap;
+    int cta = 0;
+    size_t smem = 0;
+    for (size_t i = 0; i < work.size(); i++) {
+        const LagTarget t = engine_lag_target(work[i].first->eng);
+        h[i] = LagBatchItem{t.ring, t.acc, t.E, work[i].second.table, t.status, work[i].first->maps_d, cta, 0};
+        cta += static_cast<int>(work[i].second.blocks);
+        smem = std::max(smem, work[i].second.smem);
+    }
+    const int n = static_cast<int>(work.size());
+    CUDA_TRY(cudaMemcpyAsync(d, h, sizeof(LagBatchItem) * n, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaEventRecord(s->items_ev[ring], s->stream));
+    s->items_used[ring] = true;
+    switch (J) {
+#define BATCH_CASE(JJ) \
+    case JJ: lag_batch_kernel<JJ><<<cta, kLagThreads, smem, s->stream>>>(d, n); break;
+        BATCH_CASE(4) BATCH_CASE(8) BATCH_CASE(16) BATCH_CASE(20) BATCH_CASE(24) BATCH_CASE(30) BATCH_CASE(32)
+        BATCH_CASE(64)
+#undef BATCH_CASE
+        default: return fail(DDM_ERR_STATE, "internal: no batched lag kernel for this frame count");
+    }
+    CUDA_TRY(cudaGetLastError());
+    s->launches++;
+    return DDM_OK;
+}
+
+}  // namespace
+
+extern "C" double ddm_server_clock(const ddm_server *s) {
+    if (!s) return 0.0;
+    return std::chrono::duration<double>(Clock::now() - s->t0).count();
+}
+
+extern "C" int ddm_server_open(const ddm_server_config *cfg, ddm_server **out) {
+    clear_error();
+    if (!cfg || !out) return fail(DDM_ERR_INVALID_ARG, "ddm_server_open: null argument");
+    *out = nullptr;
+    if (cfg->max_streams < 0 || cfg->results_per_stream < 0)
+        return fail(DDM_ERR_INVALID_ARG, "ddm_server_open: negative limit");
+    std::unique_ptr<ddm_server> s(new ddm_server);
+    s->device = cfg->device;
+    if (cudaSetDevice(s->device) != cudaSuccess) return fail(DDM_ERR_NO_DEVICE, "cudaSetDevice failed");
+    size_t free_b = 0, total_b = 0;
+    CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    s->budget = cfg->hbm_budget_bytes ? cfg->hbm_budget_bytes : (free_b > (2ull << 30) ? free_b - (2ull << 30) : 0);
+    if (cfg->max_streams) s->max_streams = cfg->max_streams;
+    if (cfg->results_per_stream) s->results_per_stream = cfg->results_per_stream;
+    CUDA_TRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    for (int i = 0; i < kItemRing; i++) CUDA_TRY(cudaEventCreateWithFlags(&s->items_ev[i], cudaEventDisableTiming));
+    const int attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+#define BATCH_ATTR(JJ) \
+    CUDA_TRY(cudaFuncSetAttribute(lag_batch_kernel<JJ>, static_cast<cudaFuncAttribute>(attr), kLagSmemMax));
+    BATCH_ATTR(4) BATCH_ATTR(8) BATCH_ATTR(16) BATCH_ATTR(20) BATCH_ATTR(24) BATCH_ATTR(30) BATCH_ATTR(32) BATCH_ATTR(64)
+#undef BATCH_ATTR
+    *out = s.release();
+    return DDM_OK;
+}
+
+extern "C" int ddm_server_close(ddm_server *s) {
+    if (!s) return DDM_OK;
+    cudaSetDevice(s->device);
+    cudaStreamSynchronize(s->stream);
+    for (auto &kv : s->streams) release_stream(kv.second);
+    s->streams.clear();
+    if (s->items_h) cudaFreeHost(s->items_h);
+    cudaFree(s->items_d);
+    for (cudaEvent_t ev : s->items_ev)
+        if (ev) cudaEventDestroy(ev);
+    cudaStreamDestroy(s->stream);
+    delete s;
+    return DDM_OK;
+}
+
+extern "C" int ddm_server_add_stream(ddm_server *s, const ddm_config *cfg, int *stream_id) {
+    clear_error();
+    if (!s || !cfg || !stream_id) return fail(DDM_ERR_INVALID_ARG, "ddm_server_add_stream: null argument");
+    std::lock_guard<std::mutex> g(s->lock);
+    if (cfg->estimator != DDM_EST_UNBIASED)
+        return fail(DDM_ERR_INVALID_ARG, "served streams use the unbiased estimator (open-ended, a result per chunk)");
+    if (static_cast<int>(s->streams.size()) >= s->max_streams) return fail(DDM_ERR_BUSY, "all stream slots are taken");
+    if (s->used >= s->budget) return fail(DDM_ERR_BUSY, "the server's HBM budget is in use");
+    ddm_config c = *cfg;
+    c.device = s->device;
+    c.stream = s->stream;                 // all engines queue on the server's stream
+    c.hbm_budget_bytes = s->budget - s->used;  // admission: the engine refuses if it does not fit
+    c.lag_batch_frames = 0;               // pair every chunk at once: nothing held back between steps
+    c.dump_every = 0;
+    Stream st;
+    int r = ddm_open(&c, &st.eng);
+    if (r == DDM_ERR_OUT_OF_MEMORY) return fail(DDM_ERR_BUSY, std::string("not admitted now: ") + ddm_last_error());
+    if (r) return r;
+    engine_defer_lag(st.eng, true);
+    ddm_info info;
+    ddm_get_info(st.eng, &info);
+    st.bytes = info.device_bytes;
+    st.frame_bytes = static_cast<size_t>(cfg->frame_width) * cfg->frame_height * cfg->bytes_per_pixel;
+    st.isf_size = ddm_isf_size(st.eng);
+    const LagTarget t = engine_lag_target(st.eng);
+    if (cudaMalloc(reinterpret_cast<void **>(&st.maps_d), sizeof(LagMaps)) != cudaSuccess ||
+        cudaMemcpy(st.maps_d, t.maps, sizeof(LagMaps), cudaMemcpyHostToDevice) != cudaSuccess) {
+        release_stream(st);
+        return fail(DDM_ERR_OUT_OF_MEMORY, "tensor-map copy");
+    }
+    for (int i = 0; i < s->results_per_stream; i++) {
+        auto sl = std::make_unique<Slot>();
+        sl->server = s;
+        if (cudaMallocHost(reinterpret_cast<void **>(&sl->isf_h), sizeof(double) * std::max<long>(st.isf_size, 1)) !=
+                cudaSuccess ||
+            cudaMallocHost(reinterpret_cast<void **>(&sl->status_h), sizeof(int)) != cudaSuccess) {
+            st.slots.push_back(std::move(sl));
+            release_stream(st);
+            return fail(DDM_ERR_OUT_OF_MEMORY, "pinned result buffers");
+        }
+        st.slots.push_back(std::move(sl));
+    }
+    s->used += st.bytes;
+    const int id = s->next_id++;
+    s->streams.emplace(id, std::move(st));
+    *stream_id = id;
+    return DDM_OK;
+}
+
+extern "C" int ddm_server_remove_stream(ddm_server *s, int stream_id) {
+    clear_error();
+    if (!s) return fail(DDM_ERR_INVALID_ARG, "null server");
+    std::lock_guard<std::mutex> g(s->lock);
+    auto it = s->streams.find(stream_id);
+    if (it == s->streams.end()) return fail(DDM_ERR_INVALID_ARG, "unknown stream");
+    CUDA_TRY(cudaStreamSynchronize(s->stream));  // its work in flight, and its result callbacks
+    s->used -= it->second.bytes;
+    release_stream(it->second);
+    s->streams.erase(it);
+    return DDM_OK;
+}
+
+extern "C" int ddm_server_submit(ddm_server *s, int stream_id, const void *frames, int count) {
+    clear_error();
+    if (!s || !frames || count <= 0) return fail(DDM_ERR_INVALID_ARG, "ddm_server_submit: bad argument");
+    std::lock_guard<std::mutex> g(s->lock);
+    auto it = s->streams.find(stream_id);
+    if (it == s->streams.end()) return fail(DDM_ERR_INVALID_ARG, "unknown stream");
+    Stream &st = it->second;
+    PendingChunk pc;
+    if (!st.free_bufs.empty()) {
+        pc.frames = st.free_bufs.back();
+        st.free_bufs.pop_back();
+    }
+    int r = pinned(&pc.frames, st.frame_bytes * count);
+    if (r) return r;
+    std::memcpy(pc.frames.p, frames, st.frame_bytes * count);
+    pc.count = count;
+    pc.submit_s = ddm_server_clock(s);
+    st.pending.push_back(pc);
+    st.chunks_submitted++;
+    return DDM_OK;
+}
+
+extern "C" int ddm_server_step(ddm_server *s, int *chunks_issued) {
+    clear_error();
+    if (!s) return fail(DDM_ERR_INVALID_ARG, "null server");
+    std::lock_guard<std::mutex> g(s->lock);
+    if (chunks_issued) *chunks_issued = 0;
+    std::vector<std::pair<Stream *, Slot *>> taken;
+    std::map<int, std::vector<std::pair<Stream *, DeferredLag>>> by_j;
+    // 1. each stream's next chunk: H2D copy and FFT (the engine's own stream pair), lag work deferred
+    for (auto &kv : s->streams) {
+        Stream &st = kv.second;
+        if (st.pending.empty()) continue;
+        Slot *slot = nullptr;
+        for (auto &sl : st.slots)
+            if (sl->state.load() == 0) {
+                slot = sl.get();
+                break;
+            }
+        if (!slot) continue;  // the caller has not collected earlier results yet
+        PendingChunk pc = st.pending.front();
+        st.pending.pop_front();
+        int r = ddm_submit_frames(st.eng, pc.frames.p, pc.count, 0);
+        if (r) return r;
+        slot->frames = pc.frames;
+        slot->chunk_index = st.chunks_issued++;
+        st.frames_issued += pc.count;
+        slot->frames_done = st.frames_issued;
+        slot->submit_s = pc.submit_s;
+        slot->state.store(1);
+        st.order.push_back(slot);
+        taken.emplace_back(&st, slot);
+        for (const DeferredLag &d : engine_take_deferred(st.eng)) by_j[d.J].emplace_back(&st, d);
+    }
+    // 2. one lag launch per register-frame count over every taken stream
+    for (auto &kv : by_j) {
+        int r = launch_batch(s, kv.first, kv.second);
+        if (r) return r;
+    }
+    // 3. per stream: azimuthal average, ISF and status to host, completion callback
+    for (auto &ts : taken) {
+        Stream &st = *ts.first;
+        Slot *slot = ts.second;
+        int r = engine_finalize_async(st.eng);
+        if (r) return r;
+        CUDA_TRY(cudaMemcpyAsync(slot->isf_h, engine_isf_device(st.eng), sizeof(double) * st.isf_size,
+                                 cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(slot->status_h, engine_status_device(st.eng), sizeof(int), cudaMemcpyDeviceToHost,
+                                 s->stream));
+        CUDA_TRY(cudaLaunchHostFunc(s->stream, on_result, slot));
+    }
+    if (chunks_issued) *chunks_issued = static_cast<int>(taken.size());
+    return DDM_OK;
+}
+
+extern "C" int ddm_server_poll(ddm_server *s, int stream_id, ddm_chunk_result *res, double *isf, long capacity) {
+    clear_error();
+    if (!s) return fail(DDM_ERR_INVALID_ARG, "null server");
+    std::lock_guard<std::mutex> g(s->lock);
+    auto it = s->streams.find(stream_id);
+    if (it == s->streams.end()) return fail(DDM_ERR_INVALID_ARG, "unknown stream");
+    Stream &st = it->second;
+    if (st.order.empty() || st.order.front()->state.load() != 2) return 0;
+    Slot *slot = st.order.front();
+    if (*slot->status_h != 0) return fail(DDM_ERR_CUDA, "a lag-kernel pipeline wait timed out; results are incomplete");
+    if (isf) {
+        if (capacity < st.isf_size) return fail(DDM_ERR_INVALID_ARG, "ddm_server_poll: ISF buffer too small");
+        std::memcpy(isf, slot->isf_h, sizeof(double) * st.isf_size);
+    }
+    if (res) {
+        res->chunk_index = slot->chunk_index;
+        res->frames = slot->frames_done;
+        res->submit_s = slot->submit_s;
+        res->done_s = slot->done_s.load();
+    }
+    st.order.pop_front();
+    st.free_bufs.push_back(slot->frames);
+    slot->frames = PinnedBuf();
+    slot->state.store(0);
+    return 1;
+}
+
+extern "C" int ddm_server_wait(ddm_server *s) {
+    clear_error();
+    if (!s) return fail(DDM_ERR_INVALID_ARG, "null server");
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return DDM_OK;
+}
+
+extern "C" int ddm_server_get_stats(const ddm_server *s, ddm_server_stats *info) {
+    if (!s || !info) return fail(DDM_ERR_INVALID_ARG, "bad argument");
+    std::lock_guard<std::mutex> g(s->lock);
+    info->streams = static_cast<int>(s->streams.size());
+    info->device_bytes = s->used;
+    info->budget_bytes = s->budget;
+    info->batched_launches = s->launches;
+    long pending = 0;
+    for (const auto &kv : s->streams) pending += static_cast<long>(kv.second.pending.size());
+    info->chunks_pending = pending;
+    return DDM_OK;
+}

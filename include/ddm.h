@@ -34,7 +34,8 @@ typedef enum {
     DDM_ERR_STATE = 4,         /* call not valid in the engine's current state */
     DDM_ERR_NEED_FRAMES = 5,   /* finalize needs frames that were never submitted */
     DDM_ERR_NO_DEVICE = 6,     /* no CUDA device, or not an sm_100 device */
-    DDM_ERR_IO = 7             /* file could not be read or written */
+    DDM_ERR_IO = 7,            /* file could not be read or written */
+    DDM_ERR_BUSY = 8           /* a server cannot admit the stream now; retry once streams leave */
 } ddm_status;
 
 /* How a source pixel becomes the FFT input value. */
@@ -264,6 +265,62 @@ int ddm_write_isf_file(const char *path, const double *isf_qt, const float *lamb
 int ddm_synth_video(uint64_t seed, int width, int height, int frames, int spots,
                     double spot_sigma, double amplitude, double background, double step_var,
                     double step_var_b, double noise_sd, int max_value, void *out);
+
+/* ---------------------------------------------------------------------------------
+ * Serving many streams on one GPU (no counterpart in the reference, which analyses one
+ * video per process, src/DDM.cu:268-892). A server keeps every admitted stream's engine
+ * (FFT ring, accumulators) resident and runs continuous batching: ddm_server_step takes the
+ * next pending chunk of every stream (whose earlier results have been collected), runs each
+ * stream's FFT on its own CUDA stream, then one lag-kernel launch over all of those streams'
+ * lag work, then per stream the azimuthal average and the copy of its ISF to host memory.
+ * A step returns once that work is queued; chunks submitted while it runs are taken by the
+ * next step. Every chunk gets a result (the ISF of the stream so far, as ddm_finalize +
+ * ddm_read_isf would give) with its submit and completion times on the server clock.
+ * Streams use the unbiased estimator. Calls are thread-safe (one lock per server).
+ * --------------------------------------------------------------------------------- */
+typedef struct ddm_server ddm_server;
+
+typedef struct {
+    int device;                /* CUDA device ordinal */
+    size_t hbm_budget_bytes;   /* device bytes the streams may hold; 0 = free memory - 2 GiB */
+    int max_streams;           /* 0 = 64 */
+    int results_per_stream;    /* chunks of a stream in flight or awaiting ddm_server_poll; 0 = 4 */
+} ddm_server_config;
+
+typedef struct {
+    long chunk_index;  /* 0-based chunk of the stream */
+    long frames;       /* frames of the stream analysed with this chunk */
+    double submit_s;   /* server clock when the chunk was submitted */
+    double done_s;     /* server clock when its ISF reached host memory */
+} ddm_chunk_result;
+
+typedef struct {
+    int streams;            /* admitted */
+    size_t device_bytes;    /* held by them */
+    size_t budget_bytes;
+    long batched_launches;  /* lag-kernel launches covering several streams' work */
+    long chunks_pending;    /* submitted, not yet taken by a step */
+} ddm_server_stats;
+
+int ddm_server_open(const ddm_server_config *cfg, ddm_server **out);
+int ddm_server_close(ddm_server *s);
+/* Admit a stream (cfg as for ddm_open; its device, stream, lag_batch_frames and dump_every
+ * are set by the server). DDM_ERR_BUSY: it does not fit the HBM budget or the stream
+ * limit now; retry after streams leave. */
+int ddm_server_add_stream(ddm_server *s, const ddm_config *cfg, int *stream_id);
+/* Wait for the stream's work in flight, release its device memory. */
+int ddm_server_remove_stream(ddm_server *s, int stream_id);
+/* Queue one chunk of `count` frames from host memory (copied; the buffer is free on return). */
+int ddm_server_submit(ddm_server *s, int stream_id, const void *frames, int count);
+/* One continuous-batching step; *chunks_issued = chunks taken. */
+int ddm_server_step(ddm_server *s, int *chunks_issued);
+/* The stream's oldest finished chunk: returns 1 and fills res / isf (ISF layout of
+ * ddm_read_isf, capacity >= ddm_isf_size of the stream), or 0 if none is finished. */
+int ddm_server_poll(ddm_server *s, int stream_id, ddm_chunk_result *res, double *isf, long capacity);
+/* Block until all queued GPU work is done. */
+int ddm_server_wait(ddm_server *s);
+double ddm_server_clock(const ddm_server *s);  /* seconds since ddm_server_open */
+int ddm_server_get_stats(const ddm_server *s, ddm_server_stats *stats);
 
 /* Camera .movie files (src/video_reader.cpp:64-290): open, describe, read frames. */
 typedef struct {
