@@ -325,6 +325,28 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+def run_serving(args) -> None:
+    """Serving workload (see cuda_multiddm_b200/serving_bench.py): p50/p99 chunk latency and
+    analysed frames/s at each camera rate, the highest rate whose p99 stays under the chunk
+    period, and each size's chunk latency alone through the plain path."""
+    import torch
+
+    from cuda_multiddm_b200 import serving_bench as SB
+
+    torch.cuda.set_device(0)
+    vids = SB.videos()
+    runs = [SB.run(camera_fps=f, periods=args.periods, vids=vids) for f in args.camera_fps]
+    ok = [r["camera_fps"] for r in runs if r["p99_under_period"]]
+    at30 = next((r for r in runs if r["camera_fps"] == 30.0), runs[0])
+    line = {"metric": "serving: p99 chunk latency (30-frame chunks, mixed 256^2..1024^2 streams)",
+            "value": at30["p99_latency_s"] * 1000.0, "unit": "ms", "higher_is_better": False, "n_gpus": 1,
+            "data": "synthetic", "config": {"workload": "serving_mixed_streams", "arrivals_per_period": 8,
+                                            "max_streams": 64, "chunk": 30},
+            "runs": runs, "highest_camera_fps_with_p99_under_period": max(ok) if ok else None,
+            "alone_chunk_latency_s": SB.alone_latency(vids)}
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -335,9 +357,16 @@ def main() -> None:
     ap.add_argument("--lag-batch", type=int, default=0,
                     help="frames paired per lag-kernel launch (1..64; 0 = the engine default, one launch "
                          "per 30-frame piece)")
-    ap.add_argument("--workload", choices=["multiscale", "small"], default="multiscale",
-                    help="small: 512^2 frames, scales 512..64, same taus and chunk (profiling only)")
+    ap.add_argument("--workload", choices=["multiscale", "small", "serving"], default="multiscale",
+                    help="small: 512^2 frames, scales 512..64, same taus and chunk (profiling only); "
+                         "serving: many camera streams through one server (its own JSON line)")
+    ap.add_argument("--camera-fps", type=float, nargs="+", default=[30.0, 120.0, 480.0],
+                    help="serving: camera frame rates to run (30 fps = one 30-frame chunk per second)")
+    ap.add_argument("--periods", type=float, default=20.0, help="serving: chunk periods of arrivals")
     args = ap.parse_args()
+    if args.workload == "serving":
+        run_serving(args)
+        return
     if args.workload == "small":
         globals().update(SMALL)
     if args.warmup < 3:

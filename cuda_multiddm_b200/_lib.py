@@ -55,7 +55,8 @@ class ChunkResult(C.Structure):
 
 class ServerStats(C.Structure):
     _fields_ = [("streams", C.c_int), ("device_bytes", C.c_size_t), ("budget_bytes", C.c_size_t),
-                ("batched_launches", C.c_long), ("chunks_pending", C.c_long)]
+                ("batched_launches", C.c_long), ("chunks_pending", C.c_long), ("steps", C.c_long),
+                ("step_host_s", C.c_double), ("gpu_s", C.c_double)]
 
 
 class MovieInfo(C.Structure):
@@ -89,6 +90,7 @@ SIGNATURES = {
     "ddm_server_add_stream": (C.c_int, [C.c_void_p, C.POINTER(Config), C.POINTER(C.c_int)]),
     "ddm_server_remove_stream": (C.c_int, [C.c_void_p, C.c_int]),
     "ddm_server_submit": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
+    "ddm_server_submit_pinned": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
     "ddm_server_step": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "ddm_server_poll": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(ChunkResult), C.c_void_p, C.c_long]),
     "ddm_server_wait": (C.c_int, [C.c_void_p]),

@@ -28,6 +28,7 @@
 #include "lag.cuh"
 #include "engine_internal.hpp"
 #include "lag_host.hpp"
+#include "pinned_pool.hpp"
 
 namespace ddm {
 
@@ -150,7 +151,10 @@ namespace {
 template <typename Tp>
 int dev_alloc(ddm_engine *e, Tp **p, size_t count) {
     size_t bytes = sizeof(Tp) * std::max<size_t>(count, 1);
-    cudaError_t err = cudaMalloc(reinterpret_cast<void **>(p), bytes);
+    // stream-ordered from the device's memory pool (no device-wide synchronisation when
+    // engines come and go), on the engine's private FFT stream, complete before it is used
+    cudaError_t err = cudaMallocAsync(reinterpret_cast<void **>(p), bytes, e->fft_stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(e->fft_stream);
     if (err != cudaSuccess)
         return fail(DDM_ERR_OUT_OF_MEMORY, std::string("cudaMalloc of ") + std::to_string(bytes) +
                                                " bytes failed: " + cudaGetErrorString(err));
@@ -158,26 +162,18 @@ int dev_alloc(ddm_engine *e, Tp **p, size_t count) {
     return DDM_OK;
 }
 
+// Releases everything; device memory is freed in stream order after the engine's queued
+// work, host buffers go back to the pinned pool (callers make sure no copy still reads them).
 void free_all(ddm_engine *e) {
-    cudaFree(e->ring);
-    cudaFree(e->acc);
-    cudaFree(e->tw);
-    cudaFree(e->stage);
-    cudaFree(e->tables_d);
-    cudaFree(e->chunk_beg_d);
-    cudaFree(e->chunk_end_d);
-    cudaFree(e->chunk_first_d);
-    cudaFree(e->chunk_count_d);
-    cudaFree(e->partial_d);
-    cudaFree(e->idx_d);
-    cudaFree(e->counts_d);
-    cudaFree(e->norm_d);
-    cudaFree(e->isf_d);
-    cudaFree(e->fit_d);
-    if (e->norm_h) cudaFreeHost(e->norm_h);
+    void *dev[] = {e->ring, e->acc, e->tw, e->stage, e->tables_d, e->chunk_beg_d, e->chunk_end_d,
+                   e->chunk_first_d, e->chunk_count_d, e->partial_d, e->idx_d, e->counts_d, e->norm_d,
+                   e->isf_d, e->fit_d, e->status_d};
+    cudaStream_t fs = e->stream ? e->stream : e->fft_stream;
+    for (void *p : dev)
+        if (p) cudaFreeAsync(p, fs);
+    pinned_release(e->norm_h);
     if (e->norm_ev) cudaEventDestroy(e->norm_ev);
-    cudaFree(e->status_d);
-    if (e->tables_h) cudaFreeHost(e->tables_h);
+    pinned_release(e->tables_h);
     for (int i = 0; i < kTables; i++)
         if (e->tab_ev[i]) cudaEventDestroy(e->tab_ev[i]);
     for (int g = 0; g < 3; g++)
@@ -485,8 +481,11 @@ int run_ready_iterations(ddm_engine *e, bool final_pass) {
 // C ABI
 // =================================================================================
 
-extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
-    clear_error();
+namespace {
+
+// ddm_open; with plan_only it stops after the validation and sizing and reports the device
+// bytes the engine's main buffers would take (the figure checked against the HBM budget).
+int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool plan_only) {
     if (!cfg || !out) return fail(DDM_ERR_INVALID_ARG, "ddm_open: null argument");
     *out = nullptr;
     if (!cfg->scales || !cfg->taus || !cfg->lambdas || cfg->scale_count <= 0 || cfg->tau_count <= 0 ||
@@ -601,6 +600,8 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
     e->tab_stride = lag_table_capacity(e->T, kMaxJ + e->tau_max);
     size_t need = ring_bytes + acc_bytes + stage_bytes + sizeof(double) * e->isf_size +
                   sizeof(int) * static_cast<size_t>(kTables) * e->tab_stride;
+    if (need_out) *need_out = need;
+    if (plan_only) return bail(DDM_OK);
     if (cfg->hbm_budget_bytes && need > cfg->hbm_budget_bytes)
         return bail(fail(DDM_ERR_OUT_OF_MEMORY, "engine needs " + std::to_string(need) +
                                                     " device bytes, over the budget of " +
@@ -639,12 +640,11 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
     if ((st = dev_alloc(e, &e->isf_d, e->isf_size))) return bail(st);
     if ((st = dev_alloc(e, &e->status_d, 1))) return bail(st);
     if (cudaMemset(e->status_d, 0, sizeof(int)) != cudaSuccess) return bail(fail(DDM_ERR_CUDA, "status memset failed"));
-    if (cudaMallocHost(reinterpret_cast<void **>(&e->norm_h), sizeof(double) * e->T) != cudaSuccess ||
-        cudaEventCreateWithFlags(&e->norm_ev, cudaEventDisableTiming) != cudaSuccess)
+    e->norm_h = static_cast<double *>(pinned_alloc(sizeof(double) * e->T));
+    if (!e->norm_h || cudaEventCreateWithFlags(&e->norm_ev, cudaEventDisableTiming) != cudaSuccess)
         return bail(fail(DDM_ERR_OUT_OF_MEMORY, "pinned norm buffer"));
-    if (cudaMallocHost(reinterpret_cast<void **>(&e->tables_h),
-                       sizeof(int) * static_cast<size_t>(kTables) * e->tab_stride) != cudaSuccess)
-        return bail(fail(DDM_ERR_OUT_OF_MEMORY, "pinned table buffer"));
+    e->tables_h = static_cast<int *>(pinned_alloc(sizeof(int) * static_cast<size_t>(kTables) * e->tab_stride));
+    if (!e->tables_h) return bail(fail(DDM_ERR_OUT_OF_MEMORY, "pinned table buffer"));
     for (int i = 0; i < kTables; i++)
         if (cudaEventCreateWithFlags(&e->tab_ev[i], cudaEventDisableTiming) != cudaSuccess)
             return bail(fail(DDM_ERR_CUDA, "cudaEventCreate failed"));
@@ -715,13 +715,28 @@ extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
         cudaFuncSetAttribute(lag_pipe_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess)
         return bail(fail(DDM_ERR_CUDA, "cudaFuncSetAttribute failed"));
 
+    // on a caller's stream (a server's) the memsets stay queued ahead of the engine's work
     if (cudaMemsetAsync(e->acc, 0, acc_bytes, e->stream) != cudaSuccess ||
         cudaMemsetAsync(e->ring, 0, ring_bytes, e->stream) != cudaSuccess ||
-        cudaStreamSynchronize(e->stream) != cudaSuccess)
+        (e->own_stream && cudaStreamSynchronize(e->stream) != cudaSuccess))
         return bail(fail(DDM_ERR_CUDA, "initial memset failed"));
     *out = e;
     return DDM_OK;
 }
+
+}  // namespace
+
+extern "C" int ddm_open(const ddm_config *cfg, ddm_engine **out) {
+    clear_error();
+    return open_engine(cfg, out, nullptr, false);
+}
+
+namespace ddm {
+int engine_plan_bytes(const ddm_config *cfg, size_t *need) {
+    ddm_engine *unused = nullptr;
+    return open_engine(cfg, &unused, need, true);
+}
+}  // namespace ddm
 
 extern "C" int ddm_close(ddm_engine *e) {
     if (!e) return DDM_OK;
@@ -811,6 +826,12 @@ int engine_finalize_async(ddm_engine *e) {
 }
 
 void engine_defer_lag(ddm_engine *e, bool on) { e->defer_lag = on; }
+
+void engine_close_async(ddm_engine *e) {
+    if (!e) return;
+    free_all(e);
+    delete e;
+}
 
 std::vector<DeferredLag> engine_take_deferred(ddm_engine *e) {
     std::vector<DeferredLag> out;

@@ -31,6 +31,12 @@ struct LagTarget {  // what a lag launch of this engine reads and writes
 void engine_defer_lag(ddm_engine *e, bool on);
 std::vector<DeferredLag> engine_take_deferred(ddm_engine *e);
 LagTarget engine_lag_target(const ddm_engine *e);
+// Validation and sizing of ddm_open only: the device bytes checked against the HBM budget.
+int engine_plan_bytes(const ddm_config *cfg, size_t *need);
+// ddm_close without synchronising: device memory is freed in stream order on the engine's
+// stream; the caller makes sure none of the engine's queued copies still reads its host
+// buffers (they return to the pinned pool at once).
+void engine_close_async(ddm_engine *e);
 // ddm_finalize without the device-status read and its synchronisation.
 int engine_finalize_async(ddm_engine *e);
 cudaStream_t engine_stream(const ddm_engine *e);

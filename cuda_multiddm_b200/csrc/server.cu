@@ -13,6 +13,7 @@
 #include <chrono>
 #include <cstring>
 #include <deque>
+#include <list>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -23,6 +24,7 @@
 #include "engine_internal.hpp"
 #include "errors.hpp"
 #include "lag.cuh"
+#include "pinned_pool.hpp"
 
 using namespace ddm;
 
@@ -35,6 +37,7 @@ using Clock = std::chrono::steady_clock;
 struct PinnedBuf {
     void *p = nullptr;
     size_t bytes = 0;
+    bool owned = true;  // false: the caller's page-locked buffer (ddm_server_submit_pinned)
 };
 
 struct Slot {  // one chunk on its way through the GPU, and its result
@@ -57,6 +60,7 @@ struct PendingChunk {
 
 struct Stream {
     ddm_engine *eng = nullptr;
+    cudaEvent_t gone = nullptr;  // removal: recorded after the stream's last queued work
     size_t bytes = 0;
     size_t frame_bytes = 0;
     long isf_size = 0;
@@ -79,11 +83,13 @@ void CUDART_CB on_result(void *arg) {  // runs on a CUDA driver thread: no CUDA 
 struct ddm_server {
     int device = 0;
     cudaStream_t stream = nullptr;
-    size_t budget = 0, used = 0;
+    size_t budget = 0, used = 0, reserved = 0;
+    int opening = 0;  // streams being admitted outside the lock
     int max_streams = 64, results_per_stream = 4;
     Clock::time_point t0 = Clock::now();
     int next_id = 1;
     std::map<int, Stream> streams;
+    std::list<Stream> closing;  // removed, waiting for their queued work before release
     mutable std::mutex lock;
     // batched lag descriptors
     LagBatchItem *items_h = nullptr, *items_d = nullptr;
@@ -91,9 +97,52 @@ struct ddm_server {
     cudaEvent_t items_ev[kItemRing] = {};
     bool items_used[kItemRing] = {};
     long launches = 0;
+    long steps = 0;
+    double step_host_s = 0.0, gpu_s = 0.0;
+    std::deque<std::pair<cudaEvent_t, cudaEvent_t>> step_ev;  // steps whose GPU time is not yet counted
+    std::vector<cudaEvent_t> spare_ev;
 };
 
 namespace {
+
+// Adds the GPU time of finished steps to gpu_s and recycles their events.
+void collect_step_times(ddm_server *s) {
+    while (!s->step_ev.empty() && cudaEventQuery(s->step_ev.front().second) == cudaSuccess) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, s->step_ev.front().first, s->step_ev.front().second) == cudaSuccess)
+            s->gpu_s += ms / 1000.0;
+        s->spare_ev.push_back(s->step_ev.front().first);
+        s->spare_ev.push_back(s->step_ev.front().second);
+        s->step_ev.pop_front();
+    }
+}
+
+void release_stream(Stream &st);
+
+void reap(ddm_server *s, bool wait) {
+    for (auto it = s->closing.begin(); it != s->closing.end();) {
+        Stream &st = *it;
+        if (wait || !st.gone || cudaEventQuery(st.gone) == cudaSuccess) {
+            if (wait && st.gone) cudaEventSynchronize(st.gone);
+            s->used -= st.bytes;
+            release_stream(st);
+            it = s->closing.erase(it);
+        } else {
+            ++it;
+        }
+    }
+}
+
+cudaEvent_t take_event(ddm_server *s) {
+    if (!s->spare_ev.empty()) {
+        cudaEvent_t ev = s->spare_ev.back();
+        s->spare_ev.pop_back();
+        return ev;
+    }
+    cudaEvent_t ev = nullptr;
+    if (cudaEventCreate(&ev) != cudaSuccess) return nullptr;
+    return ev;
+}
 
 #define CUDA_TRY(expr)                                                                            \
     do {                                                                                          \
@@ -101,28 +150,33 @@ namespace {
         if (err__ != cudaSuccess) return fail(DDM_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(err__)); \
     } while (0)
 
+void drop(PinnedBuf &b) {
+    if (b.owned) pinned_release(b.p);
+    b = PinnedBuf();
+}
+
 int pinned(PinnedBuf *b, size_t bytes) {
-    if (b->bytes >= bytes) return DDM_OK;
-    if (b->p) cudaFreeHost(b->p);
-    b->p = nullptr;
-    b->bytes = 0;
-    if (cudaMallocHost(&b->p, bytes) != cudaSuccess) return fail(DDM_ERR_OUT_OF_MEMORY, "pinned host buffer");
+    if (b->owned && b->bytes >= bytes && b->p) return DDM_OK;
+    drop(*b);
+    b->p = pinned_alloc(bytes);
+    if (!b->p) return fail(DDM_ERR_OUT_OF_MEMORY, "pinned host buffer");
     b->bytes = bytes;
+    b->owned = true;
     return DDM_OK;
 }
 
+// Releases a stream whose queued work has all run (its removal event has completed).
 void release_stream(Stream &st) {
-    if (st.eng) ddm_close(st.eng);
-    cudaFree(st.maps_d);
+    engine_close_async(st.eng);
+    cudaFreeAsync(st.maps_d, nullptr);
     for (auto &sl : st.slots) {
-        if (sl->isf_h) cudaFreeHost(sl->isf_h);
-        if (sl->status_h) cudaFreeHost(sl->status_h);
-        if (sl->frames.p) cudaFreeHost(sl->frames.p);
+        pinned_release(sl->isf_h);
+        pinned_release(sl->status_h);
+        drop(sl->frames);
     }
-    for (auto &pc : st.pending)
-        if (pc.frames.p) cudaFreeHost(pc.frames.p);
-    for (auto &b : st.free_bufs)
-        if (b.p) cudaFreeHost(b.p);
+    for (auto &pc : st.pending) drop(pc.frames);
+    for (auto &b : st.free_bufs) drop(b);
+    if (st.gone) cudaEventDestroy(st.gone);
     st = Stream();
 }
 
@@ -199,6 +253,21 @@ extern "C" int ddm_server_open(const ddm_server_config *cfg, ddm_server **out) {
     if (cfg->max_streams) s->max_streams = cfg->max_streams;
     if (cfg->results_per_stream) s->results_per_stream = cfg->results_per_stream;
     CUDA_TRY(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    // Keep freed stream memory in the device pool, so streams that leave make room for the
+    // next ones without a trip through the driver, and map the whole budget into the pool
+    // now: growing the pool while streams run holds up their work (measured: a p99 chunk
+    // latency of about 1 s on a cold pool against 12 ms on a warm one).
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess) {
+        uint64_t keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        void *warm = nullptr;
+        if (s->budget && cudaMallocAsync(&warm, s->budget, s->stream) == cudaSuccess) {
+            cudaFreeAsync(warm, s->stream);
+            cudaStreamSynchronize(s->stream);
+        }
+        cudaGetLastError();  // a budget the pool cannot map at once is not an error
+    }
     for (int i = 0; i < kItemRing; i++) CUDA_TRY(cudaEventCreateWithFlags(&s->items_ev[i], cudaEventDisableTiming));
     const int attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
 #define BATCH_ATTR(JJ) \
@@ -213,8 +282,21 @@ extern "C" int ddm_server_close(ddm_server *s) {
     if (!s) return DDM_OK;
     cudaSetDevice(s->device);
     cudaStreamSynchronize(s->stream);
+    for (auto &pr : s->step_ev) {
+        cudaEventDestroy(pr.first);
+        cudaEventDestroy(pr.second);
+    }
+    for (cudaEvent_t ev : s->spare_ev) cudaEventDestroy(ev);
+    reap(s, true);
     for (auto &kv : s->streams) release_stream(kv.second);
     s->streams.clear();
+    cudaStreamSynchronize(s->stream);  // the stream-ordered frees
+    cudaMemPool_t pool;  // hand the warm pool back to the device
+    if (cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess) {
+        uint64_t none = 0;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &none);
+        cudaMemPoolTrimTo(pool, 0);
+    }
     if (s->items_h) cudaFreeHost(s->items_h);
     cudaFree(s->items_d);
     for (cudaEvent_t ev : s->items_ev)
@@ -227,21 +309,42 @@ extern "C" int ddm_server_close(ddm_server *s) {
 extern "C" int ddm_server_add_stream(ddm_server *s, const ddm_config *cfg, int *stream_id) {
     clear_error();
     if (!s || !cfg || !stream_id) return fail(DDM_ERR_INVALID_ARG, "ddm_server_add_stream: null argument");
-    std::lock_guard<std::mutex> g(s->lock);
     if (cfg->estimator != DDM_EST_UNBIASED)
         return fail(DDM_ERR_INVALID_ARG, "served streams use the unbiased estimator (open-ended, a result per chunk)");
-    if (static_cast<int>(s->streams.size()) >= s->max_streams) return fail(DDM_ERR_BUSY, "all stream slots are taken");
-    if (s->used >= s->budget) return fail(DDM_ERR_BUSY, "the server's HBM budget is in use");
     ddm_config c = *cfg;
     c.device = s->device;
-    c.stream = s->stream;                 // all engines queue on the server's stream
-    c.hbm_budget_bytes = s->budget - s->used;  // admission: the engine refuses if it does not fit
-    c.lag_batch_frames = 0;               // pair every chunk at once: nothing held back between steps
+    c.stream = s->stream;      // all engines queue on the server's stream
+    c.lag_batch_frames = 0;    // pair every chunk at once: nothing held back between steps
     c.dump_every = 0;
-    Stream st;
-    int r = ddm_open(&c, &st.eng);
-    if (r == DDM_ERR_OUT_OF_MEMORY) return fail(DDM_ERR_BUSY, std::string("not admitted now: ") + ddm_last_error());
+    c.hbm_budget_bytes = 0;
+    size_t need = 0;
+    int r = engine_plan_bytes(&c, &need);
     if (r) return r;
+    // admission: reserve the stream's bytes under the lock, build its engine without it (steps
+    // of the admitted streams go on meanwhile), then insert it
+    {
+        std::lock_guard<std::mutex> g(s->lock);
+        reap(s, false);
+        if (static_cast<int>(s->streams.size()) + s->opening >= s->max_streams)
+            return fail(DDM_ERR_BUSY, "all stream slots are taken");
+        if (s->used + s->reserved + need > s->budget)
+            return fail(DDM_ERR_BUSY, "not admitted now: the stream needs " + std::to_string(need) +
+                                          " device bytes, " + std::to_string(s->budget - s->used - s->reserved) +
+                                          " of the budget are free");
+        s->reserved += need;
+        s->opening++;
+    }
+    Stream st;
+    auto unreserve = [&]() {
+        std::lock_guard<std::mutex> g(s->lock);
+        s->reserved -= need;
+        s->opening--;
+    };
+    r = ddm_open(&c, &st.eng);
+    if (r) {
+        unreserve();
+        return r == DDM_ERR_OUT_OF_MEMORY ? fail(DDM_ERR_BUSY, std::string("not admitted now: ") + ddm_last_error()) : r;
+    }
     engine_defer_lag(st.eng, true);
     ddm_info info;
     ddm_get_info(st.eng, &info);
@@ -249,22 +352,23 @@ extern "C" int ddm_server_add_stream(ddm_server *s, const ddm_config *cfg, int *
     st.frame_bytes = static_cast<size_t>(cfg->frame_width) * cfg->frame_height * cfg->bytes_per_pixel;
     st.isf_size = ddm_isf_size(st.eng);
     const LagTarget t = engine_lag_target(st.eng);
-    if (cudaMalloc(reinterpret_cast<void **>(&st.maps_d), sizeof(LagMaps)) != cudaSuccess ||
-        cudaMemcpy(st.maps_d, t.maps, sizeof(LagMaps), cudaMemcpyHostToDevice) != cudaSuccess) {
-        release_stream(st);
-        return fail(DDM_ERR_OUT_OF_MEMORY, "tensor-map copy");
-    }
-    for (int i = 0; i < s->results_per_stream; i++) {
+    bool ok = cudaMallocAsync(reinterpret_cast<void **>(&st.maps_d), sizeof(LagMaps), s->stream) == cudaSuccess &&
+              cudaMemcpyAsync(st.maps_d, t.maps, sizeof(LagMaps), cudaMemcpyHostToDevice, s->stream) == cudaSuccess;
+    for (int i = 0; ok && i < s->results_per_stream; i++) {
         auto sl = std::make_unique<Slot>();
         sl->server = s;
-        if (cudaMallocHost(reinterpret_cast<void **>(&sl->isf_h), sizeof(double) * std::max<long>(st.isf_size, 1)) !=
-                cudaSuccess ||
-            cudaMallocHost(reinterpret_cast<void **>(&sl->status_h), sizeof(int)) != cudaSuccess) {
-            st.slots.push_back(std::move(sl));
-            release_stream(st);
-            return fail(DDM_ERR_OUT_OF_MEMORY, "pinned result buffers");
-        }
+        sl->isf_h = static_cast<double *>(pinned_alloc(sizeof(double) * std::max<long>(st.isf_size, 1)));
+        sl->status_h = static_cast<int *>(pinned_alloc(sizeof(int)));
+        ok = sl->isf_h && sl->status_h;
         st.slots.push_back(std::move(sl));
+    }
+    std::lock_guard<std::mutex> g(s->lock);
+    s->reserved -= need;
+    s->opening--;
+    if (!ok) {
+        cudaStreamSynchronize(s->stream);
+        release_stream(st);
+        return fail(DDM_ERR_OUT_OF_MEMORY, "server stream buffers");
     }
     s->used += st.bytes;
     const int id = s->next_id++;
@@ -279,14 +383,24 @@ extern "C" int ddm_server_remove_stream(ddm_server *s, int stream_id) {
     std::lock_guard<std::mutex> g(s->lock);
     auto it = s->streams.find(stream_id);
     if (it == s->streams.end()) return fail(DDM_ERR_INVALID_ARG, "unknown stream");
-    CUDA_TRY(cudaStreamSynchronize(s->stream));  // its work in flight, and its result callbacks
-    s->used -= it->second.bytes;
-    release_stream(it->second);
+    // released once the server's stream has run everything queued for it (result callbacks
+    // included), without waiting here
+    Stream st = std::move(it->second);
     s->streams.erase(it);
+    if (cudaEventCreateWithFlags(&st.gone, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventRecord(st.gone, s->stream) != cudaSuccess) {
+        if (st.gone) cudaEventDestroy(st.gone);
+        st.gone = nullptr;
+        CUDA_TRY(cudaStreamSynchronize(s->stream));
+    }
+    s->closing.push_back(std::move(st));
+    reap(s, false);
     return DDM_OK;
 }
 
-extern "C" int ddm_server_submit(ddm_server *s, int stream_id, const void *frames, int count) {
+namespace {
+
+int submit_chunk(ddm_server *s, int stream_id, const void *frames, int count, bool copy) {
     clear_error();
     if (!s || !frames || count <= 0) return fail(DDM_ERR_INVALID_ARG, "ddm_server_submit: bad argument");
     std::lock_guard<std::mutex> g(s->lock);
@@ -294,13 +408,19 @@ extern "C" int ddm_server_submit(ddm_server *s, int stream_id, const void *frame
     if (it == s->streams.end()) return fail(DDM_ERR_INVALID_ARG, "unknown stream");
     Stream &st = it->second;
     PendingChunk pc;
-    if (!st.free_bufs.empty()) {
-        pc.frames = st.free_bufs.back();
-        st.free_bufs.pop_back();
+    if (copy) {
+        if (!st.free_bufs.empty()) {
+            pc.frames = st.free_bufs.back();
+            st.free_bufs.pop_back();
+        }
+        int r = pinned(&pc.frames, st.frame_bytes * count);
+        if (r) return r;
+        std::memcpy(pc.frames.p, frames, st.frame_bytes * count);
+    } else {
+        pc.frames.p = const_cast<void *>(frames);
+        pc.frames.bytes = st.frame_bytes * count;
+        pc.frames.owned = false;
     }
-    int r = pinned(&pc.frames, st.frame_bytes * count);
-    if (r) return r;
-    std::memcpy(pc.frames.p, frames, st.frame_bytes * count);
     pc.count = count;
     pc.submit_s = ddm_server_clock(s);
     st.pending.push_back(pc);
@@ -308,11 +428,28 @@ extern "C" int ddm_server_submit(ddm_server *s, int stream_id, const void *frame
     return DDM_OK;
 }
 
+}  // namespace
+
+extern "C" int ddm_server_submit(ddm_server *s, int stream_id, const void *frames, int count) {
+    return submit_chunk(s, stream_id, frames, count, true);
+}
+
+extern "C" int ddm_server_submit_pinned(ddm_server *s, int stream_id, const void *frames, int count) {
+    return submit_chunk(s, stream_id, frames, count, false);
+}
+
 extern "C" int ddm_server_step(ddm_server *s, int *chunks_issued) {
     clear_error();
     if (!s) return fail(DDM_ERR_INVALID_ARG, "null server");
     std::lock_guard<std::mutex> g(s->lock);
     if (chunks_issued) *chunks_issued = 0;
+    const auto t_start = Clock::now();
+    reap(s, false);
+    collect_step_times(s);
+    cudaEvent_t ev0 = nullptr;
+    bool any = false;
+    for (auto &kv : s->streams) any = any || !kv.second.pending.empty();
+    if (any && (ev0 = take_event(s))) CUDA_TRY(cudaEventRecord(ev0, s->stream));
     std::vector<std::pair<Stream *, Slot *>> taken;
     std::map<int, std::vector<std::pair<Stream *, DeferredLag>>> by_j;
     // 1. each stream's next chunk: H2D copy and FFT (the engine's own stream pair), lag work deferred
@@ -357,6 +494,19 @@ extern "C" int ddm_server_step(ddm_server *s, int *chunks_issued) {
                                  s->stream));
         CUDA_TRY(cudaLaunchHostFunc(s->stream, on_result, slot));
     }
+    if (ev0) {
+        cudaEvent_t ev1 = take_event(s);
+        if (ev1) {
+            CUDA_TRY(cudaEventRecord(ev1, s->stream));
+            s->step_ev.emplace_back(ev0, ev1);
+        } else {
+            s->spare_ev.push_back(ev0);
+        }
+    }
+    if (!taken.empty()) {
+        s->steps++;
+        s->step_host_s += std::chrono::duration<double>(Clock::now() - t_start).count();
+    }
     if (chunks_issued) *chunks_issued = static_cast<int>(taken.size());
     return DDM_OK;
 }
@@ -382,7 +532,7 @@ extern "C" int ddm_server_poll(ddm_server *s, int stream_id, ddm_chunk_result *r
         res->done_s = slot->done_s.load();
     }
     st.order.pop_front();
-    st.free_bufs.push_back(slot->frames);
+    if (slot->frames.owned) st.free_bufs.push_back(slot->frames);
     slot->frames = PinnedBuf();
     slot->state.store(0);
     return 1;
@@ -405,5 +555,9 @@ extern "C" int ddm_server_get_stats(const ddm_server *s, ddm_server_stats *info)
     long pending = 0;
     for (const auto &kv : s->streams) pending += static_cast<long>(kv.second.pending.size());
     info->chunks_pending = pending;
+    info->steps = s->steps;
+    info->step_host_s = s->step_host_s;
+    collect_step_times(const_cast<ddm_server *>(s));
+    info->gpu_s = s->gpu_s;
     return DDM_OK;
 }

@@ -19,8 +19,9 @@ class Server:
         h = C.c_void_p()
         check(lib().ddm_server_open(C.byref(cfg), C.byref(h)))
         self._h = h
-        self._isf_size: dict[int, int] = {}
+        self._isf: dict[int, np.ndarray] = {}  # per-stream result buffer
         self._cfgs: dict[int, EngineConfig] = {}
+        self._res = ChunkResult()
 
     def close(self) -> None:
         if self._h:
@@ -42,35 +43,42 @@ class Server:
             return None
         check(st)
         M = max(cfg.scales)
-        self._isf_size[sid.value] = sum((M // s) ** 2 for s in cfg.scales) * len(cfg.lambdas) * len(cfg.taus)
+        size = sum((M // s) ** 2 for s in cfg.scales) * len(cfg.lambdas) * len(cfg.taus)
+        self._isf[sid.value] = np.zeros(size, np.float64)
         self._cfgs[sid.value] = cfg
         return sid.value
 
     def remove_stream(self, sid: int) -> None:
         check(lib().ddm_server_remove_stream(self._h, sid))
-        self._isf_size.pop(sid, None)
+        self._isf.pop(sid, None)
         self._cfgs.pop(sid, None)
 
     def submit(self, sid: int, frames: np.ndarray) -> None:
+        """Queue a chunk (copied)."""
         f = np.ascontiguousarray(frames)
         check(lib().ddm_server_submit(self._h, sid, f.ctypes.data, int(f.shape[0])))
+
+    def submit_pinned(self, sid: int, ptr: int, count: int) -> None:
+        """Queue a chunk from page-locked memory at `ptr` (e.g. a pinned torch tensor's
+        data_ptr()) without copying; keep it unchanged until the chunk's result is polled."""
+        check(lib().ddm_server_submit_pinned(self._h, sid, C.c_void_p(ptr), count))
 
     def step(self) -> int:
         n = C.c_int()
         check(lib().ddm_server_step(self._h, C.byref(n)))
         return n.value
 
-    def poll(self, sid: int):
-        """(ChunkResult fields as a dict, ISF array) of the stream's oldest finished chunk, or None."""
-        res = ChunkResult()
-        isf = np.zeros(self._isf_size[sid], np.float64)
+    def poll(self, sid: int, copy: bool = True):
+        """(ChunkResult fields as a dict, ISF array) of the stream's oldest finished chunk, or
+        None. copy=False returns the stream's result buffer, overwritten by the next poll."""
+        res, isf = self._res, self._isf[sid]
         st = lib().ddm_server_poll(self._h, sid, C.byref(res), isf.ctypes.data, isf.size)
         if st == 0:
             return None
         if st != 1:
             raise DDMError(st, lib().ddm_last_error().decode(errors="replace"))
         return {"chunk_index": res.chunk_index, "frames": res.frames, "submit_s": res.submit_s,
-                "done_s": res.done_s, "latency_s": res.done_s - res.submit_s}, isf
+                "done_s": res.done_s, "latency_s": res.done_s - res.submit_s}, (isf.copy() if copy else isf)
 
     def wait(self) -> None:
         check(lib().ddm_server_wait(self._h))

@@ -300,6 +300,10 @@ typedef struct {
     size_t budget_bytes;
     long batched_launches;  /* lag-kernel launches covering several streams' work */
     long chunks_pending;    /* submitted, not yet taken by a step */
+    long steps;             /* ddm_server_step calls that took at least one chunk */
+    double step_host_s;     /* host time spent inside those calls */
+    double gpu_s;           /* GPU time of finished steps on the server's stream, from its first
+                               operation to its last (queueing excluded) */
 } ddm_server_stats;
 
 int ddm_server_open(const ddm_server_config *cfg, ddm_server **out);
@@ -308,10 +312,15 @@ int ddm_server_close(ddm_server *s);
  * are set by the server). DDM_ERR_BUSY: it does not fit the HBM budget or the stream
  * limit now; retry after streams leave. */
 int ddm_server_add_stream(ddm_server *s, const ddm_config *cfg, int *stream_id);
-/* Wait for the stream's work in flight, release its device memory. */
+/* Remove a stream: its device memory is released once the work queued for it has run
+ * (without waiting here); its unpolled results are dropped. */
 int ddm_server_remove_stream(ddm_server *s, int stream_id);
 /* Queue one chunk of `count` frames from host memory (copied; the buffer is free on return). */
 int ddm_server_submit(ddm_server *s, int stream_id, const void *frames, int count);
+/* As ddm_server_submit without the copy: `frames` is page-locked host memory (cudaMallocHost,
+ * cudaHostRegister) that the caller leaves unchanged until this chunk's result has been
+ * returned by ddm_server_poll. */
+int ddm_server_submit_pinned(ddm_server *s, int stream_id, const void *frames, int count);
 /* One continuous-batching step; *chunks_issued = chunks taken. */
 int ddm_server_step(ddm_server *s, int *chunks_issued);
 /* The stream's oldest finished chunk: returns 1 and fills res / isf (ISF layout of
