@@ -335,6 +335,7 @@ def run_serving(args) -> None:
 
     torch.cuda.set_device(0)
     vids = SB.videos()
+    SB.run(camera_fps=240.0, periods=6.0, vids=vids, seed=99)  # warm-up: module loads, pinned pool
     runs = [SB.run(camera_fps=f, periods=args.periods, vids=vids) for f in args.camera_fps]
     ok = [r["camera_fps"] for r in runs if r["p99_under_period"]]
     at30 = next((r for r in runs if r["camera_fps"] == 30.0), runs[0])
