@@ -302,7 +302,7 @@ def run_ours(args) -> None:
                 "config": {"workload": "multiscale_1024_4scales_64tau" if SIDE == 1024 else
                            "small_512_4scales_64tau (profiling)", "frames": N_FRAMES, "side": SIDE,
                            "scales": SCALES, "taus": T, "tau_max": max(taus), "lambdas": len(lambdas),
-                           "chunk": CHUNK, "lag_batch_frames": args.lag_batch or min(CHUNK, 32),
+                           "chunk": CHUNK, "lag_batch_frames": args.lag_batch or 32,
                            "estimator": "unbiased", "steady_state": True,
                            "l2": "inputs larger than L2 (ring of %d frames x %.1f MB)"
                                  % (eng.info().ring_slots, frames_elements() * 8 / 1e6),
@@ -356,8 +356,7 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--lag-batch", type=int, default=0,
-                    help="frames paired per lag-kernel launch (1..64; 0 = the engine default, one launch "
-                         "per 30-frame piece)")
+                    help="frames paired per lag-kernel launch (1..64; 0 = the engine default, 32)")
     ap.add_argument("--workload", choices=["multiscale", "small", "serving"], default="multiscale",
                     help="small: 512^2 frames, scales 512..64, same taus and chunk (profiling only); "
                          "serving: many camera streams through one server (its own JSON line)")

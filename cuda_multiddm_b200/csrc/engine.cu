@@ -12,6 +12,7 @@
 //   masks  int    CSR of annulus element indices per (scale, q); counts [S][Q].
 //   isf    double [sum_s tiles_s * Q * T].
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -88,6 +89,13 @@ struct ddm_engine {
     // (the ring carries one extra piece of slots for that).
     cudaStream_t fft_stream = nullptr;
     cudaEvent_t ev_fft = nullptr, ev_guard[2] = {nullptr, nullptr};
+    // Host-submitted frames: their copies into the staging buffer run on copy_stream, one FFT
+    // group at a time, so the copy of group g + 1 overlaps the FFT of group g; ev_copy orders
+    // each group's FFT after its copies, ev_stage holds the next piece's copies until the
+    // FFTs reading the staging buffer are done.
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_copy = nullptr, ev_stage = nullptr;
+    bool stage_busy = false;
     long long pieces = 0;
     int R = 0, jmax = 32;
     float2 *ring = nullptr, *acc = nullptr, *tw = nullptr;
@@ -182,6 +190,9 @@ void free_all(ddm_engine *e) {
             cudaEventDestroy(pr.second);
         }
     if (e->ev_fft) cudaEventDestroy(e->ev_fft);
+    if (e->ev_copy) cudaEventDestroy(e->ev_copy);
+    if (e->ev_stage) cudaEventDestroy(e->ev_stage);
+    if (e->copy_stream) cudaStreamDestroy(e->copy_stream);
     for (cudaEvent_t ev : e->ev_guard)
         if (ev) cudaEventDestroy(ev);
     if (e->fft_stream) cudaStreamDestroy(e->fft_stream);
@@ -215,8 +226,11 @@ struct TimedRange {
 // FFT of a piece of frames into ring slots (first_label + f) % R
 // ---------------------------------------------------------------------------------
 
+// `before_group(f0, nf)` runs before each group's kernels are queued (the host path queues the
+// group's copies there).
 int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long long row_pitch,
-               int x_off, int y_off, int nframes, long long first_label) {
+               int x_off, int y_off, int nframes, long long first_label,
+               const std::function<int(int, int)> &before_group = nullptr) {
     TimedRange tr(e, 0);
     FftArgs rows, cols;
     std::memset(&rows, 0, sizeof(rows));
@@ -265,6 +279,10 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
     const int group = static_cast<int>(std::max<long long>(1, std::min<long long>(nframes, (64LL << 20) / frame_bytes)));
     for (int f0 = 0; f0 < nframes; f0 += group) {
         const int nf = std::min(group, nframes - f0);
+        if (before_group) {
+            int st = before_group(f0, nf);
+            if (st) return st;
+        }
         rows.src = src + f0 * frame_stride;
         rows.first_label = cols.first_label = first_label + f0;
         fft_rows_kernel<<<dim3(row_ctas, nf), kFftThreads, smem, e->fft_stream>>>(rows);
@@ -572,7 +590,10 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
     e->jmax = std::min(kPieceFrames, e->C);
     if (cfg->lag_batch_frames < 0 || cfg->lag_batch_frames > kMaxJ)
         return bail(fail(DDM_ERR_INVALID_ARG, "lag_batch_frames must be 0.." + std::to_string(kMaxJ)));
-    e->lag_batch = cfg->lag_batch_frames ? cfg->lag_batch_frames : e->jmax;
+    // default: unbiased launches of kPieceFrames (32) frames, the instantiated register-frame
+    // count the kernel's cost per launch is set by (32 frames take about the time of 30);
+    // compat iterations in blocks of one ingest piece
+    e->lag_batch = cfg->lag_batch_frames ? cfg->lag_batch_frames : (compat ? e->jmax : kPieceFrames);
     if (compat) {
         e->its = compat_schedule(e->N, e->C, e->multistream, e->G, e->taus, &e->frames_read);
         // Frames arrive in pieces of jmax and iterations run in order, each once every
@@ -623,6 +644,9 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
         e->own_stream = true;
     }
     if (cudaStreamCreateWithFlags(&e->fft_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e->ev_copy, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e->ev_stage, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&e->ev_fft, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&e->ev_guard[0], cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&e->ev_guard[1], cudaEventDisableTiming) != cudaSuccess)
@@ -775,15 +799,25 @@ extern "C" int ddm_submit_frames(ddm_engine *e, const void *frames, int count, i
                             e->x_off, e->y_off, piece, e->submitted);
         } else {
             const size_t roi_row = static_cast<size_t>(e->M) * e->bpp;
-            for (int f = 0; f < piece; f++) {
-                const uint8_t *fp = p + frame_bytes * f +
-                                    (static_cast<size_t>(e->y_off) * e->w + e->x_off) * e->bpp;
-                CUDA_TRY(cudaMemcpy2DAsync(e->stage + static_cast<size_t>(f) * e->M * roi_row, roi_row, fp,
-                                           static_cast<size_t>(e->w) * e->bpp, roi_row, e->M,
-                                           cudaMemcpyHostToDevice, e->fft_stream));
-            }
+            if (e->stage_busy) CUDA_TRY(cudaStreamWaitEvent(e->copy_stream, e->ev_stage, 0));
+            auto copy_group = [&](int f0, int nf) -> int {
+                for (int f = f0; f < f0 + nf; f++) {
+                    const uint8_t *fp = p + frame_bytes * f +
+                                        (static_cast<size_t>(e->y_off) * e->w + e->x_off) * e->bpp;
+                    CUDA_TRY(cudaMemcpy2DAsync(e->stage + static_cast<size_t>(f) * e->M * roi_row, roi_row, fp,
+                                               static_cast<size_t>(e->w) * e->bpp, roi_row, e->M,
+                                               cudaMemcpyHostToDevice, e->copy_stream));
+                }
+                CUDA_TRY(cudaEventRecord(e->ev_copy, e->copy_stream));
+                CUDA_TRY(cudaStreamWaitEvent(e->fft_stream, e->ev_copy, 0));
+                return DDM_OK;
+            };
             st = launch_fft(e, e->stage, static_cast<long long>(e->M) * roi_row, static_cast<long long>(roi_row),
-                            0, 0, piece, e->submitted);
+                            0, 0, piece, e->submitted, copy_group);
+            if (!st) {
+                CUDA_TRY(cudaEventRecord(e->ev_stage, e->fft_stream));
+                e->stage_busy = true;
+            }
         }
         if (st) return st;
         CUDA_TRY(cudaEventRecord(e->ev_fft, e->fft_stream));
@@ -889,6 +923,7 @@ extern "C" int ddm_synchronize(ddm_engine *e) {
     if (!e) return fail(DDM_ERR_INVALID_ARG, "null engine");
     int st = flush_lag(e);
     if (st) return st;
+    CUDA_TRY(cudaStreamSynchronize(e->copy_stream));
     CUDA_TRY(cudaStreamSynchronize(e->fft_stream));
     CUDA_TRY(cudaStreamSynchronize(e->stream));
     CUDA_TRY(cudaGetLastError());

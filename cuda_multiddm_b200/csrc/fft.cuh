@@ -369,13 +369,13 @@ __device__ __forceinline__ void fft_cols_body(const FftArgs &a, const FftScale &
     }
 
 // grid (sum of ctas_per_frame, frames)
-__global__ void __launch_bounds__(kFftThreads, 3) fft_rows_kernel(FftArgs a) {
+__global__ void __launch_bounds__(kFftThreads, 4) fft_rows_kernel(FftArgs a) {
     extern __shared__ float2 fsm[];
     const FftScale &sc = a.sc[fft_find_scale(a)];
     DDM_FFT_DISPATCH(fft_rows_body)
 }
 
-__global__ void __launch_bounds__(kFftThreads, 3) fft_cols_kernel(FftArgs a) {
+__global__ void __launch_bounds__(kFftThreads, 4) fft_cols_kernel(FftArgs a) {
     extern __shared__ float2 fsm[];
     const FftScale &sc = a.sc[fft_find_scale(a)];
     DDM_FFT_DISPATCH(fft_cols_body)

@@ -314,7 +314,7 @@ extern "C" int ddm_server_add_stream(ddm_server *s, const ddm_config *cfg, int *
     ddm_config c = *cfg;
     c.device = s->device;
     c.stream = s->stream;      // all engines queue on the server's stream
-    c.lag_batch_frames = 0;    // pair every chunk at once: nothing held back between steps
+    c.lag_batch_frames = std::min(cfg->chunk_frames > 0 ? cfg->chunk_frames : 1, 32);  // pair every chunk at once
     c.dump_every = 0;
     c.hbm_budget_bytes = 0;
     size_t need = 0;

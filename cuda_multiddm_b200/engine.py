@@ -33,7 +33,7 @@ class EngineConfig:
     hbm_budget_bytes: int = 0
     device: int = 0
     stream: int | None = None          # a cudaStream_t as an integer, or None
-    lag_batch_frames: int = 0          # frames per lag launch (1..64; 0 = min(chunk_frames, 32))
+    lag_batch_frames: int = 0          # frames per lag launch (1..64; 0 = 32 unbiased, min(chunk_frames, 32) compat)
     _keep: list = field(default_factory=list, repr=False)
 
     def to_c(self) -> Config:

@@ -74,10 +74,11 @@ typedef struct {
     size_t hbm_budget_bytes;       /* refuse to open if the engine would need more; 0 = no limit */
     int device;                    /* CUDA device ordinal */
     void *stream;                  /* cudaStream_t to run on; NULL = the engine creates one */
-    int lag_batch_frames;          /* frames paired per lag launch, 1..64; 0 = min(C, 32),
-                                      one launch per ingest piece. Unbiased: a larger value
-                                      holds frames back for fuller launches, which read fewer
-                                      partner bytes per frame. Compat: A-frames per launch. */
+    int lag_batch_frames;          /* frames paired per lag launch, 1..64. Unbiased (0 = 32):
+                                      up to lag_batch_frames - 1 frames may wait in the ring
+                                      for a fuller launch (fuller launches read fewer partner
+                                      bytes per frame); finalize/synchronize pair them. Compat
+                                      (0 = min(C, 32)): A-frames per launch. */
 } ddm_config;
 
 typedef struct ddm_engine ddm_engine;

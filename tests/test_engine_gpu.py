@@ -107,7 +107,8 @@ def test_unbiased_multiscale_matches_oracle():
     isf, _, info = engine_run(frames, scales, taus, lambdas, estimator="unbiased", C=10)
     want, _ = O.ddm_run(frames, scales, taus, lambdas, estimator=O.EST_UNBIASED, chunk=10)
     assert_isf_close(isf, want, scales, len(lambdas), len(taus))
-    assert info.ring_slots == 55 + 2 * 10  # tau_max + one piece + one piece of FFT overlap
+    # tau_max + one piece + one piece of FFT overlap + up to 31 frames held for a 32-frame launch
+    assert info.ring_slots == 55 + 2 * 10 + 31
 
 
 def test_u16_full_precision_matches_oracle():
@@ -223,6 +224,29 @@ def test_unaveraged_and_power_spectrum_match_oracle():
             off += n
 
 
+def test_fine_scales_2048_matches_oracle():
+    """The batched-fine-scales configuration's shape at a reduced frame count: 2048^2 frames,
+    scales 2048 .. 32 (5461 tiles per frame), lambdas from 2 px to past the smallest tile."""
+    frames = media.synth_video(1003, 2048, 2048, 16, 16000, step_var=1.0)
+    scales = [2048, 1024, 512, 256, 128, 64, 32]
+    taus, lambdas = [1, 2, 5, 11], media.log_lambdas(2, 512, 12)
+    isf, _, _ = engine_run(frames, scales, taus, lambdas, estimator="unbiased", C=8)
+    want, _ = O.ddm_run(frames, scales, taus, lambdas, estimator=O.EST_UNBIASED, chunk=8)
+    assert_isf_close(isf, want, scales, len(lambdas), len(taus))
+
+
+def test_high_bit_depth_2048_matches_oracle():
+    """The high-bit-depth configuration's shape at a reduced frame count: 2048^2 uint16 holding
+    12-bit values, Poisson shot noise, two populations (D = 0.2 and 2.0 px^2/frame), scales
+    2048 .. 256, full 16-bit decoding."""
+    frames = media.synth_video(1004, 2048, 2048, 12, 8000, amplitude=2000, background=300, step_var=0.4,
+                               step_var_b=4.0, noise_sd=-1, max_value=4095)
+    scales, taus, lambdas = [2048, 1024, 512, 256], [1, 3, 8], media.log_lambdas(2, 256, 10)
+    isf, _, _ = engine_run(frames, scales, taus, lambdas, estimator="unbiased", C=6, pixel_mode="u16")
+    want, _ = O.ddm_run(frames, scales, taus, lambdas, estimator=O.EST_UNBIASED, chunk=6, pixmode=O.PIX_U16LE)
+    assert_isf_close(isf, want, scales, len(lambdas), len(taus))
+
+
 def test_errors_are_status_codes():
     base = dict(frame_width=64, frame_height=64, taus=[1, 2], lambdas=[4.0], chunk_frames=4)
     with pytest.raises(DDMError) as e:
@@ -255,6 +279,7 @@ def test_kernel_launches_counted():
     frames = media.synth_video(2, 64, 64, 8, 10)
     _, _, info = engine_run(frames, [64, 32], [1, 2], [4.0], estimator="unbiased", C=4)
     # per piece of 4 frames: one row-pass and one column-pass launch over all scales (the
-    # 4 frames fit one L2-resident group) + 1 lag launch; then the two azimuthal stages
-    assert info.kernel_launches == 2 * (2 + 1) + 2
+    # 4 frames fit one L2-resident group); the 8 frames' lag pairs in one launch at finalize
+    # (launches take up to 32 frames); then the two azimuthal stages
+    assert info.kernel_launches == 2 * 2 + 1 + 2
     assert lib() is not None

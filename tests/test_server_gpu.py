@@ -67,7 +67,9 @@ def test_each_stream_same_alone_and_in_the_mix():
 
 def test_admission_follows_the_hbm_budget():
     cfg = _cfg(256, [256, 128], [1, 2, 4], [4.0, 8.0])
-    with Engine(cfg) as eng:
+    alone = _cfg(256, [256, 128], [1, 2, 4], [4.0, 8.0])
+    alone.lag_batch_frames = C  # a served stream pairs each chunk at once
+    with Engine(alone) as eng:
         one = eng.info().device_bytes
     with Server(hbm_budget_bytes=int(2.5 * one)) as srv:
         a, b = srv.add_stream(cfg), srv.add_stream(cfg)

@@ -31,7 +31,7 @@ def test_static_lag_matches_engine_on_two_calls():
                        chunk_frames=F, estimator="unbiased")
     with Engine(cfg) as eng:
         assert eng.info().ring_slots >= 2 * F  # every frame's spectrum is still in the ring
-        eng.submit(frames)  # two pieces of F frames: two lag launches
+        eng.submit(frames)
         want = eng.accumulators()
         spectra = np.stack([eng.spectrum(f) for f in range(2 * F)])  # [frames][E] complex64
     E = spectra.shape[1]
