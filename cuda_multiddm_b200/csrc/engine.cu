@@ -739,10 +739,14 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
         cudaFuncSetAttribute(lag_pipe_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess)
         return bail(fail(DDM_ERR_CUDA, "cudaFuncSetAttribute failed"));
 
-    // on a caller's stream (a server's) the memsets stay queued ahead of the engine's work
-    if (cudaMemsetAsync(e->acc, 0, acc_bytes, e->stream) != cudaSuccess ||
-        cudaMemsetAsync(e->ring, 0, ring_bytes, e->stream) != cudaSuccess ||
-        (e->own_stream && cudaStreamSynchronize(e->stream) != cudaSuccess))
+    // Zero the accumulators on the engine's private FFT stream, ahead of its first FFT: every
+    // lag launch waits for an FFT of that stream, so nothing else has to wait here (a
+    // server's shared stream stays free while a new stream is set up). The unbiased
+    // estimator never reads a ring slot before its frame is written, so only compat mode
+    // (whose reference schedule can name frames it never wrote) clears the ring.
+    if (cudaMemsetAsync(e->acc, 0, acc_bytes, e->fft_stream) != cudaSuccess ||
+        (compat && cudaMemsetAsync(e->ring, 0, ring_bytes, e->fft_stream) != cudaSuccess) ||
+        (e->own_stream && cudaStreamSynchronize(e->fft_stream) != cudaSuccess))
         return bail(fail(DDM_ERR_CUDA, "initial memset failed"));
     *out = e;
     return DDM_OK;
@@ -974,6 +978,7 @@ extern "C" int ddm_read_accumulators(ddm_engine *e, double *out, long capacity) 
     int st = flush_lag(e);
     if (st) return st;
     std::vector<float2> tmp(static_cast<size_t>(e->T) * e->E);
+    CUDA_TRY(cudaStreamSynchronize(e->fft_stream));
     CUDA_TRY(cudaStreamSynchronize(e->stream));
     CUDA_TRY(cudaMemcpy(tmp.data(), e->acc, sizeof(float2) * tmp.size(), cudaMemcpyDeviceToHost));
     for (size_t i = 0; i < tmp.size(); i++) out[i] = static_cast<double>(tmp[i].x) - static_cast<double>(tmp[i].y);
