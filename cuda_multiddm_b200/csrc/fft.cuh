@@ -15,9 +15,12 @@
 // graphics processors", SC 2008): passes of radix 16 and one closing pass of radix 2, 4
 // or 8, each thread holding 16 values in registers per pass, natural order in and out.
 // A team of L/16 threads (1 for L < 16) owns one transform; a CTA of kFftThreads threads
-// runs 256/team transforms side by side in shared memory. Element i of a transform sits
-// at i + i/16 (one float2 of padding per 16) so the strided stores of a pass hit distinct
-// banks; transforms are kFftPad(L) elements apart.
+// runs 256/team transforms side by side in shared memory, thread tid working on transform
+// tid % (256/team) (transforms fastest: a half-warp then spans 16 transforms, or all of a
+// CTA's transforms and 16/that many team members, which with the transform stride below
+// keeps every pass and staging access free of bank conflicts at every length -- with teams
+// fastest the lengths 32..128 took two wavefronts per access). Element i of a transform
+// sits at i + i/16 (one float2 of padding per 16); transforms are kFftPad(L) elements apart.
 //
 // Every transform length is a template parameter (one instance per log2 L, chosen per scale
 // at run time), so all index arithmetic folds to constants. Twiddles come from per-length
@@ -304,11 +307,13 @@ __device__ __forceinline__ void fft_rows_body(const FftArgs &a, const FftScale &
     }
 loaded:
     __syncthreads();
-    const int c_me = threadIdx.x / TEAM, t = threadIdx.x & (TEAM - 1);
-    float2 *buf = fsm + c_me * TS;
-    fft_transform<LOG2L>(buf, t, a.tw + (L - 2));
-    // split Z = X0 + i X1 into the two real rows' half spectra
-    const int g = g0 + c_me;
+    const int c_me = threadIdx.x & (NT - 1), t = threadIdx.x / NT;  // transforms fastest (no bank conflicts)
+    fft_transform<LOG2L>(fsm + c_me * TS, t, a.tw + (L - 2));  // ends with a CTA barrier
+    // split Z = X0 + i X1 into the two real rows' half spectra, teams fastest again so that
+    // a team's consecutive threads store consecutive elements of one output row
+    const int c_out = threadIdx.x / TEAM, t_out = threadIdx.x & (TEAM - 1);
+    const float2 *buf = fsm + c_out * TS;
+    const int g = g0 + c_out;
     if (g >= total_pairs) return;
     const int tile = g >> (LOG2L - 1 > 0 ? LOG2L - 1 : 0);
     const int py = 2 * (g & (L / 2 - 1));
@@ -316,7 +321,7 @@ loaded:
     float2 *o = a.ring + slot * a.E + sc.off + tile * sc.n + static_cast<long long>(py) * NX;
 #pragma unroll
     for (int m = 0; m < (NX + TEAM - 1) / TEAM; m++) {
-        const int k = t + m * TEAM;
+        const int k = t_out + m * TEAM;
         if (k < NX) {
             const float2 zk = buf[fpad(k & (L - 1))], zm = buf[fpad((L - k) & (L - 1))];
             o[k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
@@ -350,7 +355,7 @@ __device__ __forceinline__ void fft_cols_body(const FftArgs &a, const FftScale &
         fsm[c * TS + fpad(y)] = v;
     }
     __syncthreads();
-    const int c_me = threadIdx.x / TEAM, t = threadIdx.x & (TEAM - 1);
+    const int c_me = threadIdx.x & (NT - 1), t = threadIdx.x / NT;  // transforms fastest (no bank conflicts)
     fft_transform<LOG2L>(fsm + c_me * TS, t, a.tw + (L - 2));
 #pragma unroll
     for (int it = 0; it < ITER; it++) {
