@@ -74,6 +74,7 @@ struct ddm_engine {
     float tol = 1.2f;
     int C = 30, estimator = DDM_EST_UNBIASED, multistream = 1, N = 0, G = 0, device = 0;
     int M = 0, S = 0, T = 0, Q = 0, tau_max = 0;
+    int sms = 0;  // SMs of the device (persistent lag grid)
     long long E = 0;
     std::vector<ScaleDesc> sd;
     long long isf_size = 0;
@@ -326,11 +327,13 @@ int launch_lag(ddm_engine *e, const Launch &L) {
         return DDM_OK;
     }
     TimedRange tr(e, 1);
+    // persistent grid: every resident CTA walks element blocks blockIdx.x, + gridDim.x, ...
+    const unsigned grid = std::min<unsigned>(blocks, static_cast<unsigned>(kLagCtasPerSm * e->sms));
     switch (J) {
 #define LAG_CASE(JJ)                                                                                   \
     case JJ:                                                                                           \
-        lag_pipe_kernel<JJ><<<blocks, kLagThreads, smem, e->stream>>>(e->ring, e->acc, e->E, td, e->status_d, \
-                                                                       e->maps);                        \
+        lag_pipe_kernel<JJ><<<grid, kLagThreads, smem, e->stream>>>(e->ring, e->acc, e->E, td, e->status_d, \
+                                                                     e->maps, static_cast<int>(blocks)); \
         break;
         LAG_CASE(4) LAG_CASE(8) LAG_CASE(16) LAG_CASE(20) LAG_CASE(24) LAG_CASE(30) LAG_CASE(32) LAG_CASE(64)
 #undef LAG_CASE
@@ -636,6 +639,7 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
     if (cudaGetDeviceProperties(&prop, e->device) != cudaSuccess || prop.major != 10)
         return bail(fail(DDM_ERR_NO_DEVICE, "device " + std::to_string(e->device) + " is not an sm_100 GPU"));
     if (cudaSetDevice(e->device) != cudaSuccess) return bail(fail(DDM_ERR_CUDA, "cudaSetDevice failed"));
+    e->sms = prop.multiProcessorCount;
     if (cfg->stream) {
         e->stream = static_cast<cudaStream_t>(cfg->stream);
     } else {

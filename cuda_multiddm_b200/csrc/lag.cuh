@@ -21,6 +21,13 @@
 // (FP32 sum + Kahan compensation, 8 B) are loaded three entries ahead with plain coalesced
 // loads and written back once per entry.
 //
+// Persistent grid. An engine's launch has kLagCtasPerSm CTAs per SM (or fewer, one per
+// element block), and CTA c walks element blocks c, c + gridDim.x, ...: the table, the
+// barriers and the pipeline are set up once, the producer runs into the next block's groups
+// while the consumers finish the current one (the group counter runs on across blocks, and
+// the consumers release every group of a block at its end), and as the CTAs retire the SMs
+// pass to the next piece's FFT on the other stream instead of to further lag blocks.
+//
 // Every mbarrier wait is bounded (kWaitCycles clock cycles); a wait that runs out
 // sets *status to 1, and the CTA waits (bounded again) for its own copies in flight before
 // returning, so a broken schedule ends the kernel instead of hanging the GPU.
@@ -34,6 +41,7 @@ namespace ddm {
 
 constexpr int kLagConsumerWarps = 4;
 constexpr int kLagThreads = kLagConsumerWarps * 32 + 32;  // consumers + one producer warp
+constexpr int kLagCtasPerSm = 3;  // registers (128 a thread) and shared memory (~70 KB a CTA) both allow 3
 constexpr int kLagSmemMax = 220 * 1024;
 // Register-frame counts the kernel is instantiated for (a launch uses the smallest >= nreg).
 constexpr int kLagJs[] = {4, 8, 16, 20, 24, 30, 32, 64};
@@ -160,13 +168,14 @@ struct LagMaps {
 // Group g occupies shared-memory slots [(g % kGS) * kLagGroup, +kLagGroup) with
 // kGS = lag_group_slots(J); its consecutive ring slots arrive as a few 2-D boxes (runs) that
 // all complete on full[g % kGS]; empty[g % kGS] completes when every consumer warp has moved
-// past the group. Union entry u therefore sits in shared-memory slot u % lag_ring_slots(J).
-// Neither side ever waits for the whole CTA. `block` is the CTA's element block; `maps` may
-// live in kernel parameter space or global memory.
+// past the group. Union entry u of the CTA's n-th element block (n = 0, 1, ...) therefore
+// sits in shared-memory slot (n * ngroups * kLagGroup + u) % lag_ring_slots(J). Neither side
+// ever waits for the whole CTA. The CTA handles element blocks block_begin, + block_step, ...
+// below block_end; `maps` may live in kernel parameter space or global memory.
 template <int J>
 __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, float2 *__restrict__ acc, long long E,
                                               const int *__restrict__ table, int *__restrict__ status,
-                                              const LagMaps &maps, int block) {
+                                              const LagMaps &maps, int block_begin, int block_end, int block_step) {
     constexpr int kLanes = lag_lanes(J);
     constexpr int kJT = J / kLanes;  // register frames per thread
     constexpr int kElems = lag_cta_elems(J);
@@ -181,7 +190,8 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + kRingBytes);
     uint64_t *empty = full + kGS;
     volatile int *abort_flag = reinterpret_cast<volatile int *>(empty + kGS);
-    int *tab = const_cast<int *>(reinterpret_cast<volatile int *>(abort_flag + 1));
+    volatile int *issued = abort_flag + 1;  // groups the producer has issued (running count)
+    int *tab = const_cast<int *>(reinterpret_cast<volatile int *>(abort_flag + 2));
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
@@ -193,6 +203,7 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
             mbar_init(&empty[i], kLagConsumerWarps);
         }
         *abort_flag = 0;
+        *issued = 0;
         fence_mbar_init();
     }
     __syncthreads();
@@ -205,31 +216,38 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
     const int *uslot = ent_full + ntau;
     const int *gptr = uslot + nu;
     const int *runs = gptr + ngroups + 1;
-    const long long e0 = static_cast<long long>(block) * kElems;
 
     if (warp == kLagConsumerWarps) {
-        // ---------------- producer: group g is fill g / kGS of group slot g % kGS
-        if (lane == 0) {
-            for (int g = 0; g < ngroups; g++) {
-                const int gs = g & (kGS - 1), fill = g / kGS;
+        // ---------------- producer: running group G is fill G / kGS of group slot G % kGS
+        if (lane == 0 && ngroups > 0) {
+            // group g of the CTA's element block `block`
+            long long e0 = static_cast<long long>(block_begin) * kElems;
+            for (int G = 0, g = 0, block = block_begin; block < block_end; G++) {
+                const int gs = G & (kGS - 1), fill = G / kGS;
                 if (fill > 0 && !mbar_wait_bounded(&empty[gs], (fill - 1) & 1)) {
                     *abort_flag = 1;
                     break;
                 }
                 if (*abort_flag) break;
                 const int r0 = gptr[g], r1 = gptr[g + 1];
+                *issued = G + 1;
                 if (r0 == r1) {  // no frame in the group: complete the phase without data
                     mbar_arrive(&full[gs]);
-                    continue;
+                } else {
+                    uint32_t bytes = 0;
+                    for (int r = r0; r < r1; r++) bytes += kSlotBytes << lag_run_log2rows(runs[r]);
+                    mbar_expect_tx(&full[gs], bytes);
+                    for (int r = r0; r < r1; r++) {
+                        const int run = runs[r];
+                        tma_load_2d(smem + (gs * kLagGroup + lag_run_rel(run)) * kSlotBytes,
+                                    &maps.box[kLanes - 1][lag_run_log2rows(run)], static_cast<int>(e0),
+                                    lag_run_slot(run), &full[gs]);
+                    }
                 }
-                uint32_t bytes = 0;
-                for (int r = r0; r < r1; r++) bytes += kSlotBytes << lag_run_log2rows(runs[r]);
-                mbar_expect_tx(&full[gs], bytes);
-                for (int r = r0; r < r1; r++) {
-                    const int run = runs[r];
-                    tma_load_2d(smem + (gs * kLagGroup + lag_run_rel(run)) * kSlotBytes,
-                                &maps.box[kLanes - 1][lag_run_log2rows(run)], static_cast<int>(e0), lag_run_slot(run),
-                                &full[gs]);
+                if (++g == ngroups) {
+                    g = 0;
+                    block += block_step;
+                    e0 = static_cast<long long>(block) * kElems;
                 }
             }
         }
@@ -239,85 +257,105 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
         // bank once) of one slot, so a 64-bit shared load stays at two wavefronts.
         const int h = kLanes == 2 ? (lane >> 4) : 0;
         const int m = kLanes == 2 ? warp * 16 + (lane & 15) : tid;  // element within the CTA's block
-        const long long k = e0 + m;
-        const bool valid = k < E;
-        const uint32_t toff = static_cast<uint32_t>(m) * sizeof(float2);
-        const int j0 = h * kJT;  // first register frame of this thread
-        float2 nr[kJT];          // register frames j0 .. j0 + kJT - 1, negated
+        int Gbase = 0;
+        for (int block = block_begin; block < block_end && !*abort_flag; block += block_step, Gbase += ngroups) {
+            const long long k = static_cast<long long>(block) * kElems + m;
+            const bool valid = k < E;
+            const uint32_t toff = static_cast<uint32_t>(m) * sizeof(float2);
+            const int j0 = h * kJT;  // first register frame of this thread
+            float2 nr[kJT];          // register frames j0 .. j0 + kJT - 1, negated
 #pragma unroll
-        for (int i = 0; i < kJT; i++) {
-            const int s = j0 + i < nreg ? tab[kTabReg + j0 + i] : -1;
-            const float2 v = (valid && s >= 0) ? __ldg(ring + static_cast<long long>(s) * E + k) : make_float2(0.f, 0.f);
-            nr[i] = make_float2(-v.x, -v.y);
-        }
-        const float2 zero = make_float2(0.f, 0.f);
-        float2 a0 = (valid && ntau > 0) ? acc[static_cast<long long>(ent_acc[0]) * E + k] : zero;
-        float2 a1 = (valid && ntau > 1) ? acc[static_cast<long long>(ent_acc[1]) * E + k] : zero;
-        float2 a2 = (valid && ntau > 2) ? acc[static_cast<long long>(ent_acc[2]) * E + k] : zero;
-        int waited = 0, released = 0;  // in groups; warp-uniform
-        for (int e = 0; e < ntau; e++) {
-            const float2 a3 = (valid && e + 3 < ntau) ? acc[static_cast<long long>(ent_acc[e + 3]) * E + k] : zero;
-            const int ub = ent_ub[e];
-            // Wait for every group this window reaches that no earlier window reached; groups
-            // without frames included (they complete by the producer's bare arrival), so a
-            // consumer never releases a group the producer has not issued yet. One wait per
-            // window keeps the whole window's shared-memory loads free to issue back to back.
-            const int glast = (ub + nreg - 1) >> kLagGroupLog2;
-            bool ok = true;
-            for (; waited <= glast; waited++) {
-                if (!mbar_wait_bounded(&full[waited & (kGS - 1)], (waited / kGS) & 1)) {
-                    ok = false;
+            for (int i = 0; i < kJT; i++) {
+                const int s = j0 + i < nreg ? tab[kTabReg + j0 + i] : -1;
+                const float2 v = (valid && s >= 0) ? __ldg(ring + static_cast<long long>(s) * E + k) : make_float2(0.f, 0.f);
+                nr[i] = make_float2(-v.x, -v.y);
+            }
+            const float2 zero = make_float2(0.f, 0.f);
+            float2 a0 = (valid && ntau > 0) ? acc[static_cast<long long>(ent_acc[0]) * E + k] : zero;
+            float2 a1 = (valid && ntau > 1) ? acc[static_cast<long long>(ent_acc[1]) * E + k] : zero;
+            float2 a2 = (valid && ntau > 2) ? acc[static_cast<long long>(ent_acc[2]) * E + k] : zero;
+            int waited = 0, released = 0;  // in groups; warp-uniform
+            for (int e = 0; e < ntau; e++) {
+                const float2 a3 = (valid && e + 3 < ntau) ? acc[static_cast<long long>(ent_acc[e + 3]) * E + k] : zero;
+                const int ub = ent_ub[e];
+                // Wait for every group this window reaches that no earlier window reached; groups
+                // without frames included (they complete by the producer's bare arrival), so a
+                // consumer never releases a group the producer has not issued yet. One wait per
+                // window keeps the whole window's shared-memory loads free to issue back to back.
+                const int glast = (ub + nreg - 1) >> kLagGroupLog2;
+                bool ok = true;
+                for (; waited <= glast; waited++) {
+                    const int G = Gbase + waited;
+                    if (!mbar_wait_bounded(&full[G & (kGS - 1)], (G / kGS) & 1)) {
+                        ok = false;
+                        break;
+                    }
+                }
+                if (!ok) *abort_flag = 1;
+                if (*abort_flag) break;
+                const int s0 = (Gbase * kLagGroup + ub) & (kSlots - 1);  // group G sits in group slot G % kGS
+                // byte offset of this thread's first partner: slot (s0 + j0) of the ring, element m
+                const uint32_t o = static_cast<uint32_t>((s0 + j0) & (kSlots - 1)) * kSlotBytes + toff;
+                // four independent packed accumulators (i mod 4) keep the FMA pipeline full
+                float2 acc2[4] = {zero, zero, zero, zero};
+                if (ent_full[e] && s0 + J <= kSlots) {
+                    // whole window present and contiguous in the ring: fixed offsets from one base
+                    const unsigned char *w = smem + o;
+#pragma unroll
+                    for (int i = 0; i < kJT; i++)
+                        acc2[i & 3] = f2_diff_sq_acc(*reinterpret_cast<const float2 *>(w + i * kSlotBytes), nr[i], acc2[i & 3]);
+                } else if (ent_full[e]) {  // nreg == J, every register frame and partner present
+#pragma unroll
+                    for (int i = 0; i < kJT; i++) {
+                        const uint32_t off = (o + i * kSlotBytes) & (kRingBytes - 1);  // toff < kSlotBytes survives the mask
+                        acc2[i & 3] = f2_diff_sq_acc(*reinterpret_cast<const float2 *>(smem + off), nr[i], acc2[i & 3]);
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < kJT; i++) {
+                        const int j = j0 + i;
+                        if (j < nreg && tab[kTabReg + j] >= 0 && uslot[ub + j] >= 0) {
+                            const uint32_t off = (o + i * kSlotBytes) & (kRingBytes - 1);
+                            acc2[i & 3] = f2_diff_sq_acc(*reinterpret_cast<const float2 *>(smem + off), nr[i], acc2[i & 3]);
+                        }
+                    }
+                }
+                float sum = ((acc2[0].x + acc2[0].y) + (acc2[1].x + acc2[1].y)) +
+                            ((acc2[2].x + acc2[2].y) + (acc2[3].x + acc2[3].y));
+                if (kLanes == 2) sum += __shfl_xor_sync(0xffffffffu, sum, 16);  // same value in both lanes
+                // Kahan step: a.x running sum, a.y compensation (true value a.x - a.y)
+                const float y = sum - a0.y;
+                const float t = a0.x + y;
+                a0.y = (t - a0.x) - y;
+                a0.x = t;
+                if (valid && h == 0) acc[static_cast<long long>(ent_acc[e]) * E + k] = a0;
+                a0 = a1;
+                a1 = a2;
+                a2 = a3;
+                // release the groups no later window reads (all their entries lie below the next
+                // window); after the last window every group of the block, the partial last one too
+                const int rel = e + 1 < ntau ? ent_ub[e + 1] >> kLagGroupLog2 : ngroups;
+                if (rel > released) {
+                    __syncwarp();
+                    if (lane == 0)
+                        for (int g = released; g < rel; g++) mbar_arrive(&empty[(Gbase + g) & (kGS - 1)]);
+                    released = rel;
+                }
+            }
+            if (*abort_flag) break;
+            // groups no window reached (none in tables of the host's builder): wait and release
+            for (; waited < ngroups; waited++) {
+                const int G = Gbase + waited;
+                if (!mbar_wait_bounded(&full[G & (kGS - 1)], (G / kGS) & 1)) {
+                    *abort_flag = 1;
                     break;
                 }
             }
-            if (!ok) *abort_flag = 1;
             if (*abort_flag) break;
-            const int s0 = ub & (kSlots - 1);
-            // byte offset of this thread's first partner: slot (s0 + j0) of the ring, element m
-            const uint32_t o = static_cast<uint32_t>((s0 + j0) & (kSlots - 1)) * kSlotBytes + toff;
-            // four independent packed accumulators (i mod 4) keep the FMA pipeline full
-            float2 acc2[4] = {zero, zero, zero, zero};
-            if (ent_full[e] && s0 + J <= kSlots) {
-                // whole window present and contiguous in the ring: fixed offsets from one base
-                const unsigned char *w = smem + o;
-#pragma unroll
-                for (int i = 0; i < kJT; i++)
-                    acc2[i & 3] = f2_diff_sq_acc(*reinterpret_cast<const float2 *>(w + i * kSlotBytes), nr[i], acc2[i & 3]);
-            } else if (ent_full[e]) {  // nreg == J, every register frame and partner present
-#pragma unroll
-                for (int i = 0; i < kJT; i++) {
-                    const uint32_t off = (o + i * kSlotBytes) & (kRingBytes - 1);  // toff < kSlotBytes survives the mask
-                    acc2[i & 3] = f2_diff_sq_acc(*reinterpret_cast<const float2 *>(smem + off), nr[i], acc2[i & 3]);
-                }
-            } else {
-#pragma unroll
-                for (int i = 0; i < kJT; i++) {
-                    const int j = j0 + i;
-                    if (j < nreg && tab[kTabReg + j] >= 0 && uslot[ub + j] >= 0) {
-                        const uint32_t off = (o + i * kSlotBytes) & (kRingBytes - 1);
-                        acc2[i & 3] = f2_diff_sq_acc(*reinterpret_cast<const float2 *>(smem + off), nr[i], acc2[i & 3]);
-                    }
-                }
-            }
-            float sum = ((acc2[0].x + acc2[0].y) + (acc2[1].x + acc2[1].y)) +
-                        ((acc2[2].x + acc2[2].y) + (acc2[3].x + acc2[3].y));
-            if (kLanes == 2) sum += __shfl_xor_sync(0xffffffffu, sum, 16);  // same value in both lanes
-            // Kahan step: a.x running sum, a.y compensation (true value a.x - a.y)
-            const float y = sum - a0.y;
-            const float t = a0.x + y;
-            a0.y = (t - a0.x) - y;
-            a0.x = t;
-            if (valid && h == 0) acc[static_cast<long long>(ent_acc[e]) * E + k] = a0;
-            a0 = a1;
-            a1 = a2;
-            a2 = a3;
-            // release the groups no later window reads (all their entries lie below the next window)
-            const int rel = (e + 1 < ntau ? ent_ub[e + 1] : nu) >> kLagGroupLog2;
-            if (rel > released) {
+            if (released < ngroups) {
                 __syncwarp();
                 if (lane == 0)
-                    for (int g = released; g < rel; g++) mbar_arrive(&empty[g & (kGS - 1)]);
-                released = rel;
+                    for (int g = released; g < ngroups; g++) mbar_arrive(&empty[(Gbase + g) & (kGS - 1)]);
             }
         }
     }
@@ -325,26 +363,22 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
     if (*abort_flag) {
         if (tid == 0) {
             atomicExch(status, 1);
-            // drain: wait (bounded) until every copy this CTA issued has landed
-            for (int gs = 0; gs < kGS; gs++) {
-                for (int g = gs; g < ngroups; g += kGS) {
-                    if (!mbar_try_wait(&full[gs], (g / kGS) & 1)) {
-                        mbar_wait_bounded(&full[gs], (g / kGS) & 1);
-                        break;
-                    }
-                }
-            }
+            // drain: wait (bounded) until every copy this CTA issued has landed; a group slot
+            // holds at most one fill in flight, its latest
+            const int n = *issued;
+            for (int G = n > kGS ? n - kGS : 0; G < n; G++) mbar_wait_bounded(&full[G & (kGS - 1)], (G / kGS) & 1);
         }
         __syncthreads();
     }
 }
 
-// One engine's launch: CTA b handles element block b.
+// One engine's launch: CTA b handles element blocks b, b + gridDim.x, ... below nblocks.
 template <int J>
-__global__ void __launch_bounds__(kLagThreads, 3)
+__global__ void __launch_bounds__(kLagThreads, kLagCtasPerSm)
     lag_pipe_kernel(const float2 *__restrict__ ring, float2 *__restrict__ acc, long long E,
-                    const int *__restrict__ table, int *__restrict__ status, const __grid_constant__ LagMaps maps) {
-    lag_pipe_body<J>(ring, acc, E, table, status, maps, static_cast<int>(blockIdx.x));
+                    const int *__restrict__ table, int *__restrict__ status, const __grid_constant__ LagMaps maps,
+                    int nblocks) {
+    lag_pipe_body<J>(ring, acc, E, table, status, maps, static_cast<int>(blockIdx.x), nblocks, static_cast<int>(gridDim.x));
 }
 
 // The lag work of several engines (served streams) in one launch: item i owns CTAs
@@ -362,7 +396,7 @@ struct LagBatchItem {
 };
 
 template <int J>
-__global__ void __launch_bounds__(kLagThreads, 3)
+__global__ void __launch_bounds__(kLagThreads, kLagCtasPerSm)
     lag_batch_kernel(const LagBatchItem *__restrict__ items, int n) {
     int lo = 0, hi = n - 1;  // the last item whose first CTA is at or before this one
     while (lo < hi) {
@@ -371,14 +405,15 @@ __global__ void __launch_bounds__(kLagThreads, 3)
         else hi = mid - 1;
     }
     const LagBatchItem &it = items[lo];
-    lag_pipe_body<J>(it.ring, it.acc, it.E, it.table, it.status, *it.maps, static_cast<int>(blockIdx.x) - it.cta_begin);
+    const int b = static_cast<int>(blockIdx.x) - it.cta_begin;
+    lag_pipe_body<J>(it.ring, it.acc, it.E, it.table, it.status, *it.maps, b, b + 1, 1);
 }
 
 // Dynamic shared memory of a launch of lag_pipe_kernel<J> with a table of table_ints ints
-// (1 KB of alignment slack, ring, barriers, abort flag, table).
+// (1 KB of alignment slack, ring, barriers, abort flag, issued-group count, table).
 inline size_t lag_smem_bytes(int J, int table_ints) {
     return 1024 + static_cast<size_t>(lag_ring_slots(J)) * lag_slot_bytes(J) + 2 * sizeof(uint64_t) * lag_group_slots(J) +
-           sizeof(int) * (1 + table_ints);
+           sizeof(int) * (2 + table_ints);
 }
 
 }  // namespace ddm

@@ -133,7 +133,10 @@ extern "C" int ddm_lag_accumulate_static(const void *ring, int ring_slots, long 
     float2 *a = static_cast<float2 *>(acc);
     switch (J) {
 #define LAG_CASE(JJ) \
-    case JJ: lag_pipe_kernel<JJ><<<blocks, kLagThreads, smem, s>>>(r, a, elements, d_table, d_status, maps); break;
+    case JJ:                                                                                              \
+        lag_pipe_kernel<JJ><<<blocks, kLagThreads, smem, s>>>(r, a, elements, d_table, d_status, maps,            \
+                                                              static_cast<int>(blocks));                          \
+        break;
         LAG_CASE(4) LAG_CASE(8) LAG_CASE(16) LAG_CASE(20) LAG_CASE(24) LAG_CASE(30) LAG_CASE(32)
 #undef LAG_CASE
         default: return fail(DDM_ERR_STATE, "ddm_lag_accumulate_static: no kernel for this frame count");
