@@ -17,9 +17,17 @@
 // multicast) that completes on the group's "full" mbarrier. A dedicated producer warp
 // refills a group once every consumer warp has arrived on its "empty" mbarrier. Consumers
 // wait once per window for every group it reaches, then release the groups no later window
-// reads. The |dF|^2 arithmetic uses packed FP32x2 instructions (FADD2, FFMA2). Accumulators
-// (FP32 sum + Kahan compensation, 8 B) are loaded three entries ahead with plain coalesced
-// loads and written back once per entry.
+// reads. The |dF|^2 arithmetic is a packed FP32x2 add (FADD2) and two scalar FMAs per pair.
+// Accumulators (FP32 sum + Kahan compensation, 8 B) are loaded three entries ahead with
+// plain coalesced loads and written back once per entry.
+//
+// Fused runs. With the register frames in registers and the partners in shared memory, the
+// kernel is bound by its shared-memory loads (one 8-byte load per pair) as much as by HBM:
+// without any arithmetic the ring alone streams at the copy bandwidth. Taus one frame apart
+// (1, 2, 3, ... in a log-spaced list) have windows one union entry apart, so four such
+// entries are paired in one pass over the span of their windows: each partner value is
+// loaded once and paired with up to four register frames (35 loads for 128 pairs instead
+// of 128), one accumulator per entry.
 //
 // Persistent grid. An engine's launch has kLagCtasPerSm CTAs per SM (or fewer, one per
 // element block), and CTA c walks element blocks c, c + gridDim.x, ...: the table, the
@@ -53,6 +61,12 @@ constexpr int kLagMaxJ = 64;
 constexpr int kLagGroupLog2 = 3;
 constexpr int kLagGroup = 1 << kLagGroupLog2;
 constexpr int kLagRunKinds = 4;  // box heights 1, 2, 4, 8
+// Consecutive tau entries whose windows start one union entry apart (taus one frame apart)
+// are paired kLagFuse at a time: each partner value is read from shared memory once and
+// paired with up to kLagFuse register frames (entry e + r pairs window position q with
+// register frame q - r). Table flag bits per entry: 1 = full window, 2 = first of a run.
+constexpr int kLagFuse = 4;
+constexpr int kLagFullFlag = 1, kLagRunFlag = 2;
 
 // Geometry of the kernel instantiated for J register frames per element. Up to 32 frames one
 // consumer thread owns an element and holds all J frames in registers; for 64 frames two
@@ -163,7 +177,8 @@ struct LagMaps {
     CUtensorMap box[2][kLagRunKinds];
 };
 
-// Warp-specialised pipeline over groups of kLagGroup union entries. Warps
+// Warp-specialised pipeline over groups of kLagGroup union entries. A run of kLagFuse
+// entries (table flag kLagRunFlag) is one pass over the span of its windows. Warps
 // 0..kLagConsumerWarps-1 consume; the last warp produces (its lane 0 issues the copies).
 // Group g occupies shared-memory slots [(g % kGS) * kLagGroup, +kLagGroup) with
 // kGS = lag_group_slots(J); its consecutive ring slots arrive as a few 2-D boxes (runs) that
@@ -275,14 +290,16 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
             float2 a1 = (valid && ntau > 1) ? acc[static_cast<long long>(ent_acc[1]) * E + k] : zero;
             float2 a2 = (valid && ntau > 2) ? acc[static_cast<long long>(ent_acc[2]) * E + k] : zero;
             int waited = 0, released = 0;  // in groups; warp-uniform
-            for (int e = 0; e < ntau; e++) {
+            for (int e = 0; e < ntau;) {
+                const int flags = ent_full[e];
+                const int nrun = (flags & kLagRunFlag) ? kLagFuse : 1;  // entries handled in this pass
                 const float2 a3 = (valid && e + 3 < ntau) ? acc[static_cast<long long>(ent_acc[e + 3]) * E + k] : zero;
                 const int ub = ent_ub[e];
-                // Wait for every group this window reaches that no earlier window reached; groups
-                // without frames included (they complete by the producer's bare arrival), so a
-                // consumer never releases a group the producer has not issued yet. One wait per
-                // window keeps the whole window's shared-memory loads free to issue back to back.
-                const int glast = (ub + nreg - 1) >> kLagGroupLog2;
+                // Wait for every group this window (or run of windows) reaches that no earlier
+                // window reached; groups without frames included (they complete by the producer's
+                // bare arrival), so a consumer never releases a group the producer has not issued
+                // yet. One wait per window keeps its shared-memory loads free to issue back to back.
+                const int glast = (ub + nrun - 1 + nreg - 1) >> kLagGroupLog2;
                 bool ok = true;
                 for (; waited <= glast; waited++) {
                     const int G = Gbase + waited;
@@ -296,45 +313,91 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
                 const int s0 = (Gbase * kLagGroup + ub) & (kSlots - 1);  // group G sits in group slot G % kGS
                 // byte offset of this thread's first partner: slot (s0 + j0) of the ring, element m
                 const uint32_t o = static_cast<uint32_t>((s0 + j0) & (kSlots - 1)) * kSlotBytes + toff;
-                // four independent packed accumulators (i mod 4) keep the FMA pipeline full
-                float2 acc2[4] = {zero, zero, zero, zero};
-                if (ent_full[e] && s0 + J <= kSlots) {
-                    // whole window present and contiguous in the ring: fixed offsets from one base
-                    const unsigned char *w = smem + o;
+                if (nrun == kLagFuse) {
+                    static_assert(kLagFuse == 4, "the run consumes the four prefetched accumulators");
+                    // entries e .. e + 3, windows ub .. ub + 3: position q of the run's span (one
+                    // shared-memory load) pairs with register frame q - r of entry e + r; one
+                    // packed accumulator per entry
+                    float2 c[kLagFuse] = {zero, zero, zero, zero};
+                    if (s0 + J + kLagFuse - 1 <= kSlots) {
+                        const unsigned char *w = smem + o;
 #pragma unroll
-                    for (int i = 0; i < kJT; i++)
-                        acc2[i & 3] = f2_diff_sq_acc(*reinterpret_cast<const float2 *>(w + i * kSlotBytes), nr[i], acc2[i & 3]);
-                } else if (ent_full[e]) {  // nreg == J, every register frame and partner present
+                        for (int q = 0; q < kJT + kLagFuse - 1; q++) {
+                            const float2 b = *reinterpret_cast<const float2 *>(w + q * kSlotBytes);
 #pragma unroll
-                    for (int i = 0; i < kJT; i++) {
-                        const uint32_t off = (o + i * kSlotBytes) & (kRingBytes - 1);  // toff < kSlotBytes survives the mask
-                        acc2[i & 3] = f2_diff_sq_acc(*reinterpret_cast<const float2 *>(smem + off), nr[i], acc2[i & 3]);
-                    }
-                } else {
+                            for (int r = 0; r < kLagFuse; r++)
+                                if (q - r >= 0 && q - r < kJT) c[r] = f2_diff_sq_acc(b, nr[q - r], c[r]);
+                        }
+                    } else {
 #pragma unroll
-                    for (int i = 0; i < kJT; i++) {
-                        const int j = j0 + i;
-                        if (j < nreg && tab[kTabReg + j] >= 0 && uslot[ub + j] >= 0) {
-                            const uint32_t off = (o + i * kSlotBytes) & (kRingBytes - 1);
-                            acc2[i & 3] = f2_diff_sq_acc(*reinterpret_cast<const float2 *>(smem + off), nr[i], acc2[i & 3]);
+                        for (int q = 0; q < kJT + kLagFuse - 1; q++) {
+                            const uint32_t off = (o + q * kSlotBytes) & (kRingBytes - 1);
+                            const float2 b = *reinterpret_cast<const float2 *>(smem + off);
+#pragma unroll
+                            for (int r = 0; r < kLagFuse; r++)
+                                if (q - r >= 0 && q - r < kJT) c[r] = f2_diff_sq_acc(b, nr[q - r], c[r]);
                         }
                     }
+                    float sum[kLagFuse];
+#pragma unroll
+                    for (int r = 0; r < kLagFuse; r++) {
+                        sum[r] = c[r].x + c[r].y;
+                        if (kLanes == 2) sum[r] += __shfl_xor_sync(0xffffffffu, sum[r], 16);
+                    }
+                    float2 ar[kLagFuse] = {a0, a1, a2, a3};
+#pragma unroll
+                    for (int r = 0; r < kLagFuse; r++) {
+                        const float y = sum[r] - ar[r].y;
+                        const float t = ar[r].x + y;
+                        ar[r].y = (t - ar[r].x) - y;
+                        ar[r].x = t;
+                        if (valid && h == 0) acc[static_cast<long long>(ent_acc[e + r]) * E + k] = ar[r];
+                    }
+                    a0 = (valid && e + 4 < ntau) ? acc[static_cast<long long>(ent_acc[e + 4]) * E + k] : zero;
+                    a1 = (valid && e + 5 < ntau) ? acc[static_cast<long long>(ent_acc[e + 5]) * E + k] : zero;
+                    a2 = (valid && e + 6 < ntau) ? acc[static_cast<long long>(ent_acc[e + 6]) * E + k] : zero;
+                } else {
+                    // one window; four independent packed accumulators (i mod 4) keep the FMA pipeline full
+                    float2 acc2[4] = {zero, zero, zero, zero};
+                    if ((flags & kLagFullFlag) && s0 + J <= kSlots) {
+                        // whole window present and contiguous in the ring: fixed offsets from one base
+                        const unsigned char *w = smem + o;
+#pragma unroll
+                        for (int i = 0; i < kJT; i++)
+                            acc2[i & 3] = f2_diff_sq_acc(*reinterpret_cast<const float2 *>(w + i * kSlotBytes), nr[i], acc2[i & 3]);
+                    } else if (flags & kLagFullFlag) {  // nreg == J, every register frame and partner present
+#pragma unroll
+                        for (int i = 0; i < kJT; i++) {
+                            const uint32_t off = (o + i * kSlotBytes) & (kRingBytes - 1);  // toff < kSlotBytes survives the mask
+                            acc2[i & 3] = f2_diff_sq_acc(*reinterpret_cast<const float2 *>(smem + off), nr[i], acc2[i & 3]);
+                        }
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < kJT; i++) {
+                            const int j = j0 + i;
+                            if (j < nreg && tab[kTabReg + j] >= 0 && uslot[ub + j] >= 0) {
+                                const uint32_t off = (o + i * kSlotBytes) & (kRingBytes - 1);
+                                acc2[i & 3] = f2_diff_sq_acc(*reinterpret_cast<const float2 *>(smem + off), nr[i], acc2[i & 3]);
+                            }
+                        }
+                    }
+                    float sum = ((acc2[0].x + acc2[0].y) + (acc2[1].x + acc2[1].y)) +
+                                ((acc2[2].x + acc2[2].y) + (acc2[3].x + acc2[3].y));
+                    if (kLanes == 2) sum += __shfl_xor_sync(0xffffffffu, sum, 16);  // same value in both lanes
+                    // Kahan step: a.x running sum, a.y compensation (true value a.x - a.y)
+                    const float y = sum - a0.y;
+                    const float t = a0.x + y;
+                    a0.y = (t - a0.x) - y;
+                    a0.x = t;
+                    if (valid && h == 0) acc[static_cast<long long>(ent_acc[e]) * E + k] = a0;
+                    a0 = a1;
+                    a1 = a2;
+                    a2 = a3;
                 }
-                float sum = ((acc2[0].x + acc2[0].y) + (acc2[1].x + acc2[1].y)) +
-                            ((acc2[2].x + acc2[2].y) + (acc2[3].x + acc2[3].y));
-                if (kLanes == 2) sum += __shfl_xor_sync(0xffffffffu, sum, 16);  // same value in both lanes
-                // Kahan step: a.x running sum, a.y compensation (true value a.x - a.y)
-                const float y = sum - a0.y;
-                const float t = a0.x + y;
-                a0.y = (t - a0.x) - y;
-                a0.x = t;
-                if (valid && h == 0) acc[static_cast<long long>(ent_acc[e]) * E + k] = a0;
-                a0 = a1;
-                a1 = a2;
-                a2 = a3;
+                e += nrun;
                 // release the groups no later window reads (all their entries lie below the next
                 // window); after the last window every group of the block, the partial last one too
-                const int rel = e + 1 < ntau ? ent_ub[e + 1] >> kLagGroupLog2 : ngroups;
+                const int rel = e < ntau ? ent_ub[e] >> kLagGroupLog2 : ngroups;
                 if (rel > released) {
                     __syncwarp();
                     if (lane == 0)

@@ -48,6 +48,17 @@ inline std::string build_lag_table(int nreg, const int *reg, const std::vector<i
         for (int j = 0; j < nreg && f; j++) f = uslot[ub[i] + j] >= 0;
         full[i] = f ? 1 : 0;
     }
+    // runs of kLagFuse full entries whose windows start one union entry apart
+    for (int i = 0; i + kLagFuse <= ntau;) {
+        bool run = true;
+        for (int r = 0; r < kLagFuse && run; r++) run = full[i + r] && ub[i + r] == ub[i] + r;
+        if (run) {
+            full[i] |= kLagRunFlag;
+            i += kLagFuse;
+        } else {
+            i++;
+        }
+    }
     const int ngroups = (nu + kLagGroup - 1) / kLagGroup;
     std::vector<int> gptr(ngroups + 1, 0), runs;
     for (int g = 0; g < ngroups; g++) {

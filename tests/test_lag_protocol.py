@@ -4,7 +4,8 @@ The lag kernel (cuda_multiddm_b200/csrc/lag.cuh) streams the distinct partner fr
 launch (the "union") through groups of 8 shared-memory slots (8 groups for up to 32
 register frames, 16 for 64): one producer lane issues each group's 2-D TMA boxes and arms
 the group's *full* barrier; four consumer warps wait once per window on every group it
-reaches and arrive on a group's *empty* barrier once no later window reads it. These tests build the tables with the engine's own C++ builder
+reaches and arrive on a group's *empty* barrier once no later window reads it. These tests
+build the tables with the engine's own C++ builder
 (``build_lag_table``, csrc/lag_host.hpp, driven by tests/lag_table_probe.cu) for the
 schedules the engine launches — causal windows (unbiased estimator) and the reference's
 start|end windows (src/DDM.cu:250-255) — plus random windows with holes, and check
@@ -14,8 +15,9 @@ start|end windows (src/DDM.cu:250-255) — plus random windows with holes, and c
 * the "full window" flag is right (it selects the kernel's unchecked fast paths),
 * the table fits the kernel's shared-memory limit,
 * a replay of the barrier protocol (mbarrier phase parity as the hardware defines it) under
-  random interleavings of the producer and the four consumer warps neither deadlocks nor
-  lets a consumer read a slot that holds another group's data.
+  random interleavings of the producer and the four consumer warps, over one element block
+  and over several (the persistent grid walks many per CTA, the group counter running on),
+  neither deadlocks nor lets a consumer read a slot that holds another group's data.
 """
 from __future__ import annotations
 
@@ -35,6 +37,7 @@ PROBE = ROOT / "tests" / "_build" / "lag_table_probe"
 
 # constants of csrc/lag.cuh
 GROUP, CONSUMERS = 8, 4
+FUSE, FULL_FLAG, RUN_FLAG = 4, 1, 2
 LAG_JS = (4, 8, 16, 20, 24, 30, 32, 64)
 SMEM_MAX = 220 * 1024
 TAB_ENTRIES = 5 + 64
@@ -168,7 +171,17 @@ def check_table(case: dict, d: dict) -> None:
             assert ub[e] > ub[e - 1]
         assert us[ub[e]:ub[e] + nreg] == case["pos"][w:w + nreg]
         full = nreg == J and all(r >= 0 for r in case["reg"][:nreg]) and all(s >= 0 for s in us[ub[e]:ub[e] + nreg])
-        assert d["full"][e] == int(full)
+        assert d["full"][e] & FULL_FLAG == int(full)
+    # fused runs: greedy, FUSE full entries whose windows start one union entry apart
+    e, starts = 0, set()
+    while e + FUSE <= len(ub):
+        if all(d["full"][e + r] & FULL_FLAG and ub[e + r] == ub[e] + r for r in range(FUSE)):
+            starts.add(e)
+            e += FUSE
+        else:
+            e += 1
+    assert {e for e in range(len(ub)) if d["full"][e] & RUN_FLAG} == starts
+    assert all(f & ~(FULL_FLAG | RUN_FLAG) == 0 for f in d["full"])
     # the union holds each window position once: its size is the number of distinct positions
     covered = set()
     for w in case["ent_w"]:
@@ -187,7 +200,7 @@ def check_table(case: dict, d: dict) -> None:
     assert seen == {u for u in range(nu) if us[u] >= 0}
     ntab = TAB_ENTRIES + 3 * d["ntau"] + nu + d["ngroups"] + 1 + len(d["runs"])
     slots = ring_slots(J)
-    assert 1024 + slots * slot_bytes(J) + 2 * 8 * (slots // GROUP) + 4 * (1 + ntab) <= SMEM_MAX
+    assert 1024 + slots * slot_bytes(J) + 2 * 8 * (slots // GROUP) + 4 * (2 + ntab) <= SMEM_MAX
 
 
 def parity_done(completed: int, parity: int) -> bool:
@@ -195,22 +208,42 @@ def parity_done(completed: int, parity: int) -> bool:
     return completed >= 1 and (completed - 1) % 2 == parity
 
 
-def replay(d: dict, seed: int, skip_empty_waits: bool = False) -> str:
-    """Random interleaving of the producer lane and the consumer warps, as lag_pipe_kernel:
-    a consumer waits once per window for every group up to the window's last, reads the
-    window, then releases the groups below the next window. ``skip_empty_waits`` plants the
-    protocol error the kernel avoids (not waiting on groups without frames)."""
+def replay(d: dict, seed: int, skip_empty_waits: bool = False, blocks: int = 1,
+           one_block_slots: bool = False) -> str:
+    """Random interleaving of the producer lane and the consumer warps, as lag_pipe_kernel
+    walking ``blocks`` element blocks of one launch (its persistent grid): the producer issues
+    group g of block n as running group G = n * ngroups + g into group slot G % slots; a
+    consumer waits once per window for every group up to the window's last, reads the window
+    (union entry u of block n sits in the slot of running group n * ngroups + u // 8), releases
+    the groups below the next window, and at the end of a block waits for and releases every
+    group of the block. ``skip_empty_waits`` and ``one_block_slots`` plant errors the kernel
+    avoids: not waiting on groups without frames, and looking for union entry u of every
+    block in the slot of group u // 8 (the rule for a single block)."""
     rnd = random.Random(seed)
     nreg, ntau, nu, ngroups, ub = d["nreg"], d["ntau"], d["nu"], d["ngroups"], d["ub"]
     gslots = ring_slots(pick_j(nreg)) // GROUP
     empty_groups = {g for g in range(ngroups) if d["gptr"][g] == d["gptr"][g + 1]}
     full_c, empty_c, empty_arr = [0] * gslots, [0] * gslots, [0] * gslots
-    content = [None] * gslots  # which group a group slot holds
+    content = [None] * gslots  # which running group a group slot holds
     g_next = 0
-    warps = [{"e": 0, "waited": 0, "released": 0} for _ in range(CONSUMERS)]
+    warps = [{"b": 0, "e": 0, "waited": 0, "released": 0} for _ in range(CONSUMERS)]
+
+    def landed(base: int, groups) -> bool:
+        return all(parity_done(full_c[(base + g) % gslots], ((base + g) // gslots) & 1) for g in groups
+                   if not (skip_empty_waits and g in empty_groups))
+
+    def release(s: dict, base: int, upto: int) -> None:
+        for g in range(s["released"], upto):
+            gs = (base + g) % gslots
+            empty_arr[gs] += 1
+            if empty_arr[gs] == CONSUMERS:
+                empty_arr[gs] = 0
+                empty_c[gs] += 1
+        s["released"] = max(s["released"], upto)
+
     idle = 0
     while True:
-        actors = (["P"] if g_next < ngroups else []) + [w for w in range(CONSUMERS) if warps[w]["e"] < ntau]
+        actors = (["P"] if g_next < blocks * ngroups else []) + [w for w in range(CONSUMERS) if warps[w]["b"] < blocks]
         if not actors:
             return "ok"
         a = rnd.choice(actors)
@@ -224,25 +257,27 @@ def replay(d: dict, seed: int, skip_empty_waits: bool = False) -> str:
                 progressed = True
         else:
             s = warps[a]
+            base = s["b"] * ngroups
             e = s["e"]
-            glast = (ub[e] + nreg - 1) // GROUP
-            need = [g for g in range(s["waited"], glast + 1) if not (skip_empty_waits and g in empty_groups)]
-            if all(parity_done(full_c[g % gslots], (g // gslots) & 1) for g in need):
-                s["waited"] = max(s["waited"], glast + 1)
-                for j in range(nreg):
-                    u = ub[e] + j
-                    if d["uslot"][u] >= 0 and d["reg"][j] >= 0 and content[(u // GROUP) % gslots] != u // GROUP:
-                        return f"stale read of union entry {u} by entry {e}"
-                upto = (ub[e + 1] if e + 1 < ntau else nu) // GROUP
-                for g in range(s["released"], upto):
-                    gs = g % gslots
-                    empty_arr[gs] += 1
-                    if empty_arr[gs] == CONSUMERS:
-                        empty_arr[gs] = 0
-                        empty_c[gs] += 1
-                s["released"] = max(s["released"], upto)
-                s["e"] += 1
-                progressed = True
+            if e == ntau:  # end of the block: every group waited for and released
+                if landed(base, range(s["waited"], ngroups)):
+                    release(s, base, ngroups)
+                    s.update(b=s["b"] + 1, e=0, waited=0, released=0)
+                    progressed = True
+            else:
+                nrun = FUSE if d["full"][e] & RUN_FLAG else 1  # a fused run waits once for its span
+                glast = (ub[e + nrun - 1] + nreg - 1) // GROUP
+                if landed(base, range(s["waited"], glast + 1)):
+                    s["waited"] = max(s["waited"], glast + 1)
+                    for r in range(nrun):
+                        for j in range(nreg):
+                            u = ub[e + r] + j
+                            slot = (u // GROUP if one_block_slots else base + u // GROUP) % gslots
+                            if d["uslot"][u] >= 0 and d["reg"][j] >= 0 and content[slot] != base + u // GROUP:
+                                return f"stale read of union entry {u} by entry {e + r} of block {s['b']}"
+                    s["e"] += nrun
+                    release(s, base, ub[s["e"]] // GROUP if s["e"] < ntau else ngroups)
+                    progressed = True
         idle = 0 if progressed else idle + 1
         if idle > 4000:
             return "deadlock"
@@ -257,6 +292,7 @@ def test_tables_and_protocol(probe):
         check_table(case, d)
         for seed in range(2):
             assert replay(d, seed) == "ok", (i, seed)
+            assert replay(d, seed, blocks=3) == "ok", (i, seed)
 
 
 def test_windows_must_ascend(probe):
@@ -294,3 +330,14 @@ def test_ring_must_hold_a_full_window(probe, monkeypatch):
     assert replay(d, 0) == "ok"
     monkeypatch.setattr(sys.modules[__name__], "ring_slots", lambda J: 64)
     assert replay(d, 0) == "deadlock"
+
+
+def test_block_offset_is_needed(probe):
+    """Over several element blocks a group of block n lands in the slot of running group
+    n * ngroups + g: a consumer that looked for union entry u in slot u // 8 (the one-block
+    rule) reads other groups' data whenever ngroups is not a multiple of the group slots."""
+    d = parse(build_tables(probe, [causal_case(log_taus(1, 500, 64), 1000, 32, 700)])[0])
+    assert d["ngroups"] % (ring_slots(32) // GROUP) != 0
+    assert replay(d, 0, blocks=3) == "ok"
+    assert replay(d, 0, blocks=1, one_block_slots=True) == "ok"
+    assert replay(d, 0, blocks=3, one_block_slots=True).startswith("stale read")
