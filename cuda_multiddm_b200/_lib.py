@@ -72,6 +72,8 @@ SIGNATURES = {
     "ddm_finalize": (C.c_int, [C.c_void_p]),
     "ddm_isf_size": (C.c_long, [C.c_void_p]),
     "ddm_read_isf": (C.c_int, [C.c_void_p, C.c_void_p, C.c_long]),
+    "ddm_finalize_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_long]),
+    "ddm_wait_isf": (C.c_int, [C.c_void_p]),
     "ddm_dump_count": (C.c_int, [C.c_void_p]),
     "ddm_read_dump": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_long]),
     "ddm_reset_accumulators": (C.c_int, [C.c_void_p]),

@@ -111,8 +111,22 @@ struct ddm_engine {
     double *partial_d = nullptr;                                 // stage-1 azimuthal sums
     long long az_items = 0;
     double *norm_d = nullptr, *isf_d = nullptr;
-    double *norm_h = nullptr;               // pinned source of the norm upload
-    cudaEvent_t norm_ev = nullptr;          // that upload has read norm_h
+    // norm uploads alternate between two pinned halves, so a finalize never waits for the
+    // previous one's upload (which runs after that finalize's lag work)
+    double *norm_h = nullptr;                // pinned sources of the norm upload, 2 x T
+    cudaEvent_t norm_ev[2] = {nullptr, nullptr};  // the upload from half i has read it
+    int norm_slot = 0;
+    // ddm_finalize_async results alternate between two slots: the status word copied with
+    // the result, the event after both copies, and whether it has been waited for
+    int *async_status_h = nullptr;           // pinned, 2 ints
+    cudaEvent_t async_ev[2] = {nullptr, nullptr};
+    bool async_pending[2] = {false, false};
+    int async_slot = 0;                      // slot of the next result
+    // their copies run on result_stream, so the next chunk's lag work does not queue behind
+    // them; ev_isf_ready orders a copy after its azimuthal average, ev_isf_read holds the
+    // next azimuthal average (which rewrites isf_d) until the copy has read it
+    cudaStream_t result_stream = nullptr;
+    cudaEvent_t ev_isf_ready = nullptr, ev_isf_read = nullptr;
     double *fit_d = nullptr;                // ISF fitting: means, tau, q, curve fits, D (first fit call)
     int *status_d = nullptr;                // set by kernels whose bounded waits ran out
     LagMaps maps;                           // 2-D tensor maps of the ring for the lag kernel
@@ -174,6 +188,7 @@ int dev_alloc(ddm_engine *e, Tp **p, size_t count) {
 // Releases everything; device memory is freed in stream order after the engine's queued
 // work, host buffers go back to the pinned pool (callers make sure no copy still reads them).
 void free_all(ddm_engine *e) {
+    if (e->stream && e->ev_isf_read) cudaStreamWaitEvent(e->stream, e->ev_isf_read, 0);  // a result copy reads isf_d
     void *dev[] = {e->ring, e->acc, e->tw, e->stage, e->tables_d, e->chunk_beg_d, e->chunk_end_d,
                    e->chunk_first_d, e->chunk_count_d, e->partial_d, e->idx_d, e->counts_d, e->norm_d,
                    e->isf_d, e->fit_d, e->status_d};
@@ -181,7 +196,11 @@ void free_all(ddm_engine *e) {
     for (void *p : dev)
         if (p) cudaFreeAsync(p, fs);
     pinned_release(e->norm_h);
-    if (e->norm_ev) cudaEventDestroy(e->norm_ev);
+    pinned_release(e->async_status_h);
+    for (int i = 0; i < 2; i++) {
+        if (e->norm_ev[i]) cudaEventDestroy(e->norm_ev[i]);
+        if (e->async_ev[i]) cudaEventDestroy(e->async_ev[i]);
+    }
     pinned_release(e->tables_h);
     for (int i = 0; i < kTables; i++)
         if (e->tab_ev[i]) cudaEventDestroy(e->tab_ev[i]);
@@ -194,6 +213,9 @@ void free_all(ddm_engine *e) {
     if (e->ev_copy) cudaEventDestroy(e->ev_copy);
     if (e->ev_stage) cudaEventDestroy(e->ev_stage);
     if (e->copy_stream) cudaStreamDestroy(e->copy_stream);
+    if (e->ev_isf_ready) cudaEventDestroy(e->ev_isf_ready);
+    if (e->ev_isf_read) cudaEventDestroy(e->ev_isf_read);
+    if (e->result_stream) cudaStreamDestroy(e->result_stream);
     for (cudaEvent_t ev : e->ev_guard)
         if (ev) cudaEventDestroy(ev);
     if (e->fft_stream) cudaStreamDestroy(e->fft_stream);
@@ -416,11 +438,16 @@ int lag_iteration(ddm_engine *e, const CompatIteration &it) {
 }
 
 int run_azimuth(ddm_engine *e, const std::vector<double> &norm) {
-    // the upload reads norm_h asynchronously: refill it only once the previous one has run
-    CUDA_TRY(cudaEventSynchronize(e->norm_ev));
-    std::copy(norm.begin(), norm.end(), e->norm_h);
-    CUDA_TRY(cudaMemcpyAsync(e->norm_d, e->norm_h, sizeof(double) * e->T, cudaMemcpyHostToDevice, e->stream));
-    CUDA_TRY(cudaEventRecord(e->norm_ev, e->stream));
+    // the upload reads its pinned half asynchronously: refill a half only once its previous
+    // upload (two finalizes ago) has run
+    CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_isf_read, 0));  // a result copy may still read isf_d
+    const int ns = e->norm_slot;
+    e->norm_slot ^= 1;
+    double *nh = e->norm_h + static_cast<size_t>(ns) * e->T;
+    CUDA_TRY(cudaEventSynchronize(e->norm_ev[ns]));
+    std::copy(norm.begin(), norm.end(), nh);
+    CUDA_TRY(cudaMemcpyAsync(e->norm_d, nh, sizeof(double) * e->T, cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(cudaEventRecord(e->norm_ev[ns], e->stream));
     e->host_norm = norm;
     AzArgs a;
     std::memset(&a, 0, sizeof(a));
@@ -649,6 +676,9 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
     }
     if (cudaStreamCreateWithFlags(&e->fft_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&e->result_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e->ev_isf_ready, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e->ev_isf_read, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&e->ev_copy, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&e->ev_stage, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&e->ev_fft, cudaEventDisableTiming) != cudaSuccess ||
@@ -668,9 +698,13 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
     if ((st = dev_alloc(e, &e->isf_d, e->isf_size))) return bail(st);
     if ((st = dev_alloc(e, &e->status_d, 1))) return bail(st);
     if (cudaMemset(e->status_d, 0, sizeof(int)) != cudaSuccess) return bail(fail(DDM_ERR_CUDA, "status memset failed"));
-    e->norm_h = static_cast<double *>(pinned_alloc(sizeof(double) * e->T));
-    if (!e->norm_h || cudaEventCreateWithFlags(&e->norm_ev, cudaEventDisableTiming) != cudaSuccess)
-        return bail(fail(DDM_ERR_OUT_OF_MEMORY, "pinned norm buffer"));
+    e->norm_h = static_cast<double *>(pinned_alloc(sizeof(double) * 2 * e->T));
+    e->async_status_h = static_cast<int *>(pinned_alloc(sizeof(int) * 2));
+    if (!e->norm_h || !e->async_status_h) return bail(fail(DDM_ERR_OUT_OF_MEMORY, "pinned norm and status buffers"));
+    for (int i = 0; i < 2; i++)
+        if (cudaEventCreateWithFlags(&e->norm_ev[i], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&e->async_ev[i], cudaEventDisableTiming) != cudaSuccess)
+            return bail(fail(DDM_ERR_CUDA, "cudaEventCreate failed"));
     e->tables_h = static_cast<int *>(pinned_alloc(sizeof(int) * static_cast<size_t>(kTables) * e->tab_stride));
     if (!e->tables_h) return bail(fail(DDM_ERR_OUT_OF_MEMORY, "pinned table buffer"));
     for (int i = 0; i < kTables; i++)
@@ -772,6 +806,7 @@ int engine_plan_bytes(const ddm_config *cfg, size_t *need) {
 
 extern "C" int ddm_close(ddm_engine *e) {
     if (!e) return DDM_OK;
+    if (e->result_stream) cudaStreamSynchronize(e->result_stream);
     if (e->fft_stream) cudaStreamSynchronize(e->fft_stream);
     if (e->stream) cudaStreamSynchronize(e->stream);
     free_all(e);
@@ -899,6 +934,47 @@ extern "C" int ddm_finalize(ddm_engine *e) {
 
 extern "C" long ddm_isf_size(const ddm_engine *e) { return e ? static_cast<long>(e->isf_size) : 0; }
 
+// Waits for the ddm_finalize_async result in `slot` and checks the device status word
+// copied with it (the status of every kernel queued before that result).
+static int wait_async_slot(ddm_engine *e, int slot) {
+    if (!e->async_pending[slot]) return DDM_OK;
+    e->async_pending[slot] = false;
+    CUDA_TRY(cudaEventSynchronize(e->async_ev[slot]));
+    if (e->async_status_h[slot] != 0)
+        return fail(DDM_ERR_CUDA, "a lag-kernel pipeline wait timed out (device status " +
+                                      std::to_string(e->async_status_h[slot]) + "); results are incomplete");
+    return DDM_OK;
+}
+
+extern "C" int ddm_finalize_async(ddm_engine *e, double *out, long capacity) {
+    clear_error();
+    if (!e || !out || capacity < e->isf_size) return fail(DDM_ERR_INVALID_ARG, "ddm_finalize_async: bad argument");
+    const int slot = e->async_slot;
+    int st = wait_async_slot(e, slot);  // two results ago: already waited for by the call after it
+    if (st) return st;
+    // queue this result first, so the stream never idles while the host waits below
+    if ((st = engine_finalize_async(e))) return st;
+    CUDA_TRY(cudaEventRecord(e->ev_isf_ready, e->stream));
+    CUDA_TRY(cudaStreamWaitEvent(e->result_stream, e->ev_isf_ready, 0));
+    CUDA_TRY(cudaMemcpyAsync(out, e->isf_d, sizeof(double) * e->isf_size, cudaMemcpyDeviceToHost, e->result_stream));
+    CUDA_TRY(cudaMemcpyAsync(e->async_status_h + slot, e->status_d, sizeof(int), cudaMemcpyDeviceToHost,
+                             e->result_stream));
+    CUDA_TRY(cudaEventRecord(e->async_ev[slot], e->result_stream));
+    CUDA_TRY(cudaEventRecord(e->ev_isf_read, e->result_stream));
+    e->async_pending[slot] = true;
+    e->async_slot = slot ^ 1;
+    return wait_async_slot(e, slot ^ 1);  // the previous result: its buffer is the caller's again
+}
+
+extern "C" int ddm_wait_isf(ddm_engine *e) {
+    clear_error();
+    if (!e) return fail(DDM_ERR_INVALID_ARG, "ddm_wait_isf: null engine");
+    const int older = e->async_slot;  // the slot of the next result holds the older one, if any
+    int st = wait_async_slot(e, older);
+    int st2 = wait_async_slot(e, older ^ 1);
+    return st ? st : st2;
+}
+
 extern "C" int ddm_read_isf(ddm_engine *e, double *out, long capacity) {
     clear_error();
     if (!e || !out || capacity < e->isf_size) return fail(DDM_ERR_INVALID_ARG, "ddm_read_isf: bad argument");
@@ -934,6 +1010,7 @@ extern "C" int ddm_synchronize(ddm_engine *e) {
     CUDA_TRY(cudaStreamSynchronize(e->copy_stream));
     CUDA_TRY(cudaStreamSynchronize(e->fft_stream));
     CUDA_TRY(cudaStreamSynchronize(e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->result_stream));
     CUDA_TRY(cudaGetLastError());
     return check_device_status(e);
 }

@@ -115,6 +115,23 @@ class Engine:
     def finalize(self) -> None:
         check(lib().ddm_finalize(self._h))
 
+    def finalize_async(self, out: np.ndarray) -> None:
+        """Queue finalize and an asynchronous copy of the ISF into `out` (float64, at least
+        isf_size; pinned memory, e.g. pinned_isf_buffer(), overlaps the copy with later
+        submits). `out` holds the result after wait_isf() or the next finalize_async()."""
+        if out.dtype != np.float64 or not out.flags.c_contiguous or out.size < self.isf_size:
+            raise ValueError("finalize_async needs a contiguous float64 buffer of isf_size values")
+        check(lib().ddm_finalize_async(self._h, out.ctypes.data, out.size))
+
+    def wait_isf(self) -> None:
+        check(lib().ddm_wait_isf(self._h))
+
+    def pinned_isf_buffer(self) -> np.ndarray:
+        """A page-locked float64 buffer of isf_size values (the array keeps its pinned
+        tensor alive)."""
+        import torch
+        return torch.empty(self.isf_size, dtype=torch.float64).pin_memory().numpy()
+
     def synchronize(self) -> None:
         check(lib().ddm_synchronize(self._h))
 

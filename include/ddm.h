@@ -117,6 +117,21 @@ long ddm_isf_size(const ddm_engine *e);
  * (ascending)], into host memory (waits for the engine's stream). */
 int ddm_read_isf(ddm_engine *e, double *isf_out, long capacity);
 
+/* ddm_finalize + ddm_read_isf without stopping the stream: queues the finalize work and an
+ * asynchronous copy of its result into `isf_out` (capacity >= ddm_isf_size; pinned host
+ * memory for a copy that overlaps later work, pageable memory makes the call wait for it)
+ * and returns. Frames submitted afterwards are paired after the copied result, so a caller
+ * can submit chunk k+1 while the result of chunk k is on its way -- the rolling -G dump
+ * (src/DDM.cu:800-826) without the pause of the chunk loop. The call queues its result and
+ * then waits for the previous call's, so on return the previous buffer holds its result and
+ * is the caller's again, and one result is in flight. Unbiased estimator: any number of
+ * times; compat: once, as ddm_finalize. */
+int ddm_finalize_async(ddm_engine *e, double *isf_out, long capacity);
+
+/* Block until the last ddm_finalize_async result is in its buffer; returns DDM_ERR_CUDA if
+ * a kernel queued before it reported a failure (the status ddm_finalize checks). */
+int ddm_wait_isf(ddm_engine *e);
+
 /* -G snapshots (src/DDM.cu:800-826): number of snapshots taken so far, and a copy of
  * snapshot `index` in the ddm_read_isf layout. */
 int ddm_dump_count(const ddm_engine *e);

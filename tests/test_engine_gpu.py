@@ -186,6 +186,53 @@ def test_lag_batch_sizes_agree():
         assert_isf_close(o, out[0], scales, len(lambdas), len(taus), rtol=2e-6)
 
 
+def test_fused_tau_runs_match_oracle():
+    """Taus one frame apart are paired four entries per pass (one shared-memory load per
+    partner for up to four register frames): 1..13 gives three fused runs and single
+    entries around them. Launches of 4, 16, 30, 32 and 64 frames (the one- and two-lane
+    kernels; the 120-frame stream in 10-frame pieces puts the runs' spans across the ring's
+    wrap in some launches) against the oracle."""
+    frames = media.synth_video(47, 64, 64, 120, 30, step_var=1.0)
+    scales, taus, lambdas = [64, 32], list(range(1, 14)) + [20, 31], [3.0, 6.0, 12.0, 24.0]
+    want, _ = O.ddm_run(frames, scales, taus, lambdas, estimator=O.EST_UNBIASED, chunk=10)
+    for lb in (4, 16, 30, 32, 64):
+        isf, _, _ = engine_run(frames, scales, taus, lambdas, estimator="unbiased", C=10, lag_batch=lb)
+        assert_isf_close(isf, want, scales, len(lambdas), len(taus))
+
+
+def test_finalize_async_matches_finalize():
+    """A live result per chunk through ddm_finalize_async, the next chunk submitted while the
+    result is on its way, equals ddm_finalize + ddm_read_isf after every chunk bit for bit
+    (pinned and pageable buffers); a short buffer is an argument error."""
+    frames = media.synth_video(48, 128, 128, 90, 40, step_var=1.0)
+    kw = dict(frame_width=128, frame_height=128, scales=[128, 64], taus=[1, 2, 3, 4, 7, 12, 25],
+              lambdas=[3.0, 6.0, 12.0, 24.0], chunk_frames=15, estimator="unbiased")
+    with Engine(EngineConfig(**kw)) as eng:
+        want = []
+        for c0 in range(0, 90, 15):
+            eng.submit(frames[c0:c0 + 15])
+            eng.finalize()
+            want.append(eng.isf())
+    for pinned in (True, False):
+        with Engine(EngineConfig(**kw)) as eng:
+            bufs = [eng.pinned_isf_buffer() if pinned else np.zeros(eng.isf_size) for _ in range(2)]
+            got = []
+            for k, c0 in enumerate(range(0, 90, 15)):
+                eng.submit(frames[c0:c0 + 15])
+                eng.finalize_async(bufs[k % 2])
+                if k:  # finalize_async(k) waited for result k - 1
+                    got.append(bufs[(k - 1) % 2].copy())
+            eng.wait_isf()
+            got.append(bufs[5 % 2].copy())
+            eng.wait_isf()  # nothing pending: returns at once
+            for g, w in zip(got, want):
+                assert np.array_equal(g, w)
+            with pytest.raises(ValueError):
+                eng.finalize_async(np.zeros(eng.isf_size - 1))
+            short = np.zeros(eng.isf_size)
+            assert lib().ddm_finalize_async(eng._h, short.ctypes.data, eng.isf_size - 1) == 1  # DDM_ERR_INVALID_ARG
+
+
 def test_compat_long_chunk_matches_oracle():
     """C = 100 with lag_batch_frames = 64: each reference iteration pairs 100 A-frames, run as
     a 64-frame launch and a 36-frame launch of the 64-frame kernel (the partial-window path);
