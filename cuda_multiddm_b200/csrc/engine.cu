@@ -102,7 +102,12 @@ struct ddm_engine {
     float2 *ring = nullptr, *acc = nullptr, *tw = nullptr;
     uint8_t *stage = nullptr;
     int *tables_d = nullptr, *tables_h = nullptr;
-    cudaEvent_t tab_ev[kTables] = {};
+    cudaEvent_t tab_ev[kTables] = {};    // table slot i uploaded (its pinned host copy is free again)
+    cudaEvent_t tab_free[kTables] = {};  // the launch that read device table slot i is done
+    // Small uploads (lag tables, norms) run on upload_stream as soon as they are built, and the
+    // engine's stream waits for them: queued in stream order, a few KB could sit behind the
+    // next chunk's frame copies on the copy engine when the stream reached them.
+    cudaStream_t upload_stream = nullptr;
     bool tab_used[kTables] = {};
     int tab_stride = 0, tab_next = 0;
     int *idx_d = nullptr, *counts_d = nullptr;                  // annulus CSR indices, pixel counts
@@ -110,11 +115,12 @@ struct ddm_engine {
     int *chunk_first_d = nullptr, *chunk_count_d = nullptr;      // per (scale, q)
     double *partial_d = nullptr;                                 // stage-1 azimuthal sums
     long long az_items = 0;
-    double *norm_d = nullptr, *isf_d = nullptr;
+    double *norm_d = nullptr, *isf_d = nullptr;  // norm_d: two halves of T, alternating like norm_h
     // norm uploads alternate between two pinned halves, so a finalize never waits for the
     // previous one's upload (which runs after that finalize's lag work)
     double *norm_h = nullptr;                // pinned sources of the norm upload, 2 x T
-    cudaEvent_t norm_ev[2] = {nullptr, nullptr};  // the upload from half i has read it
+    cudaEvent_t norm_ev[2] = {nullptr, nullptr};    // the upload from half i has read it
+    cudaEvent_t norm_free[2] = {nullptr, nullptr};  // the azimuthal average that read device half i is done
     int norm_slot = 0;
     // ddm_finalize_async results alternate between two slots: the status word copied with
     // the result, the event after both copies, and whether it has been waited for
@@ -188,6 +194,7 @@ int dev_alloc(ddm_engine *e, Tp **p, size_t count) {
 // Releases everything; device memory is freed in stream order after the engine's queued
 // work, host buffers go back to the pinned pool (callers make sure no copy still reads them).
 void free_all(ddm_engine *e) {
+    if (e->upload_stream) cudaStreamSynchronize(e->upload_stream);  // uploads read pinned buffers freed below
     if (e->stream && e->ev_isf_read) cudaStreamWaitEvent(e->stream, e->ev_isf_read, 0);  // a result copy reads isf_d
     void *dev[] = {e->ring, e->acc, e->tw, e->stage, e->tables_d, e->chunk_beg_d, e->chunk_end_d,
                    e->chunk_first_d, e->chunk_count_d, e->partial_d, e->idx_d, e->counts_d, e->norm_d,
@@ -199,11 +206,14 @@ void free_all(ddm_engine *e) {
     pinned_release(e->async_status_h);
     for (int i = 0; i < 2; i++) {
         if (e->norm_ev[i]) cudaEventDestroy(e->norm_ev[i]);
+        if (e->norm_free[i]) cudaEventDestroy(e->norm_free[i]);
         if (e->async_ev[i]) cudaEventDestroy(e->async_ev[i]);
     }
     pinned_release(e->tables_h);
-    for (int i = 0; i < kTables; i++)
+    for (int i = 0; i < kTables; i++) {
         if (e->tab_ev[i]) cudaEventDestroy(e->tab_ev[i]);
+        if (e->tab_free[i]) cudaEventDestroy(e->tab_free[i]);
+    }
     for (int g = 0; g < 3; g++)
         for (auto &pr : e->tev[g]) {
             cudaEventDestroy(pr.first);
@@ -216,6 +226,7 @@ void free_all(ddm_engine *e) {
     if (e->ev_isf_ready) cudaEventDestroy(e->ev_isf_ready);
     if (e->ev_isf_read) cudaEventDestroy(e->ev_isf_read);
     if (e->result_stream) cudaStreamDestroy(e->result_stream);
+    if (e->upload_stream) cudaStreamDestroy(e->upload_stream);
     for (cudaEvent_t ev : e->ev_guard)
         if (ev) cudaEventDestroy(ev);
     if (e->fft_stream) cudaStreamDestroy(e->fft_stream);
@@ -338,8 +349,15 @@ int launch_lag(ddm_engine *e, const Launch &L) {
     int *th = e->tables_h + static_cast<size_t>(ts) * e->tab_stride;
     std::copy(table.begin(), table.end(), th);
     int *td = e->tables_d + static_cast<size_t>(ts) * e->tab_stride;
-    CUDA_TRY(cudaMemcpyAsync(td, th, sizeof(int) * ntab, cudaMemcpyHostToDevice, e->stream));
-    CUDA_TRY(cudaEventRecord(e->tab_ev[ts], e->stream));
+    if (e->defer_lag) {  // a server launches the lag work on the engine's stream later: upload in its order
+        CUDA_TRY(cudaMemcpyAsync(td, th, sizeof(int) * ntab, cudaMemcpyHostToDevice, e->stream));
+        CUDA_TRY(cudaEventRecord(e->tab_ev[ts], e->stream));
+    } else {  // ahead of the stream, once the launch that last read the device slot is done
+        CUDA_TRY(cudaStreamWaitEvent(e->upload_stream, e->tab_free[ts], 0));
+        CUDA_TRY(cudaMemcpyAsync(td, th, sizeof(int) * ntab, cudaMemcpyHostToDevice, e->upload_stream));
+        CUDA_TRY(cudaEventRecord(e->tab_ev[ts], e->upload_stream));
+        CUDA_TRY(cudaStreamWaitEvent(e->stream, e->tab_ev[ts], 0));
+    }
     e->tab_used[ts] = true;
 
     const unsigned blocks = static_cast<unsigned>((e->E + lag_cta_elems(J) - 1) / lag_cta_elems(J));
@@ -362,6 +380,7 @@ int launch_lag(ddm_engine *e, const Launch &L) {
         default: return fail(DDM_ERR_STATE, "internal: no lag kernel for this frame count");
     }
     CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaEventRecord(e->tab_free[ts], e->stream));
     tr.end(1);
     e->launches++;
     return DDM_OK;
@@ -438,16 +457,20 @@ int lag_iteration(ddm_engine *e, const CompatIteration &it) {
 }
 
 int run_azimuth(ddm_engine *e, const std::vector<double> &norm) {
-    // the upload reads its pinned half asynchronously: refill a half only once its previous
-    // upload (two finalizes ago) has run
     CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_isf_read, 0));  // a result copy may still read isf_d
+    // the upload reads its pinned half asynchronously: refill a half only once its previous
+    // upload (two finalizes ago) has run; the upload into the device half waits for the
+    // azimuthal average that last read it
     const int ns = e->norm_slot;
     e->norm_slot ^= 1;
     double *nh = e->norm_h + static_cast<size_t>(ns) * e->T;
+    double *nd = e->norm_d + static_cast<size_t>(ns) * e->T;
     CUDA_TRY(cudaEventSynchronize(e->norm_ev[ns]));
     std::copy(norm.begin(), norm.end(), nh);
-    CUDA_TRY(cudaMemcpyAsync(e->norm_d, nh, sizeof(double) * e->T, cudaMemcpyHostToDevice, e->stream));
-    CUDA_TRY(cudaEventRecord(e->norm_ev[ns], e->stream));
+    CUDA_TRY(cudaStreamWaitEvent(e->upload_stream, e->norm_free[ns], 0));
+    CUDA_TRY(cudaMemcpyAsync(nd, nh, sizeof(double) * e->T, cudaMemcpyHostToDevice, e->upload_stream));
+    CUDA_TRY(cudaEventRecord(e->norm_ev[ns], e->upload_stream));
+    CUDA_TRY(cudaStreamWaitEvent(e->stream, e->norm_ev[ns], 0));
     e->host_norm = norm;
     AzArgs a;
     std::memset(&a, 0, sizeof(a));
@@ -463,7 +486,7 @@ int run_azimuth(ddm_engine *e, const std::vector<double> &norm) {
     a.chunk_first = e->chunk_first_d;
     a.chunk_count = e->chunk_count_d;
     a.counts = e->counts_d;
-    a.norm = e->norm_d;
+    a.norm = nd;
     a.partial = e->partial_d;
     a.isf = e->isf_d;
     a.items = e->az_items;
@@ -476,10 +499,9 @@ int run_azimuth(ddm_engine *e, const std::vector<double> &norm) {
     }
     azimuth_final_kernel<<<static_cast<unsigned>((a.bins + kAzThreads - 1) / kAzThreads), kAzThreads, 0, e->stream>>>(a);
     CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaEventRecord(e->norm_free[ns], e->stream));
     tr.end(a.items > 0 ? 2 : 1);
     e->launches += a.items > 0 ? 2 : 1;
-    // pageable source: make sure the copy has consumed host_norm before it can change
-    CUDA_TRY(cudaStreamSynchronize(e->stream));
     return DDM_OK;
 }
 
@@ -677,6 +699,7 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
     if (cudaStreamCreateWithFlags(&e->fft_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&e->result_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&e->upload_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&e->ev_isf_ready, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&e->ev_isf_read, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&e->ev_copy, cudaEventDisableTiming) != cudaSuccess ||
@@ -694,7 +717,7 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
     if ((st = dev_alloc(e, &e->acc, static_cast<size_t>(e->T) * e->E))) return bail(st);
     if ((st = dev_alloc(e, &e->stage, stage_bytes))) return bail(st);
     if ((st = dev_alloc(e, &e->tables_d, static_cast<size_t>(kTables) * e->tab_stride))) return bail(st);
-    if ((st = dev_alloc(e, &e->norm_d, e->T))) return bail(st);
+    if ((st = dev_alloc(e, &e->norm_d, 2 * e->T))) return bail(st);
     if ((st = dev_alloc(e, &e->isf_d, e->isf_size))) return bail(st);
     if ((st = dev_alloc(e, &e->status_d, 1))) return bail(st);
     if (cudaMemset(e->status_d, 0, sizeof(int)) != cudaSuccess) return bail(fail(DDM_ERR_CUDA, "status memset failed"));
@@ -703,12 +726,14 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
     if (!e->norm_h || !e->async_status_h) return bail(fail(DDM_ERR_OUT_OF_MEMORY, "pinned norm and status buffers"));
     for (int i = 0; i < 2; i++)
         if (cudaEventCreateWithFlags(&e->norm_ev[i], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&e->norm_free[i], cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&e->async_ev[i], cudaEventDisableTiming) != cudaSuccess)
             return bail(fail(DDM_ERR_CUDA, "cudaEventCreate failed"));
     e->tables_h = static_cast<int *>(pinned_alloc(sizeof(int) * static_cast<size_t>(kTables) * e->tab_stride));
     if (!e->tables_h) return bail(fail(DDM_ERR_OUT_OF_MEMORY, "pinned table buffer"));
     for (int i = 0; i < kTables; i++)
-        if (cudaEventCreateWithFlags(&e->tab_ev[i], cudaEventDisableTiming) != cudaSuccess)
+        if (cudaEventCreateWithFlags(&e->tab_ev[i], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&e->tab_free[i], cudaEventDisableTiming) != cudaSuccess)
             return bail(fail(DDM_ERR_CUDA, "cudaEventCreate failed"));
 
     // FFT twiddle tables (FP64 math rounded to FP32), one per transform length
