@@ -30,6 +30,7 @@
 #include "engine_internal.hpp"
 #include "lag_host.hpp"
 #include "pinned_pool.hpp"
+#include "stream_pool.hpp"
 
 namespace ddm {
 
@@ -222,15 +223,15 @@ void free_all(ddm_engine *e) {
     if (e->ev_fft) cudaEventDestroy(e->ev_fft);
     if (e->ev_copy) cudaEventDestroy(e->ev_copy);
     if (e->ev_stage) cudaEventDestroy(e->ev_stage);
-    if (e->copy_stream) cudaStreamDestroy(e->copy_stream);
+    stream_release(e->device, e->copy_stream);
     if (e->ev_isf_ready) cudaEventDestroy(e->ev_isf_ready);
     if (e->ev_isf_read) cudaEventDestroy(e->ev_isf_read);
-    if (e->result_stream) cudaStreamDestroy(e->result_stream);
-    if (e->upload_stream) cudaStreamDestroy(e->upload_stream);
+    stream_release(e->device, e->result_stream);
+    stream_release(e->device, e->upload_stream);
     for (cudaEvent_t ev : e->ev_guard)
         if (ev) cudaEventDestroy(ev);
-    if (e->fft_stream) cudaStreamDestroy(e->fft_stream);
-    if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
+    stream_release(e->device, e->fft_stream);
+    if (e->own_stream) stream_release(e->device, e->stream);
 }
 
 // Brackets a group of launches with events when timing is on (group 0 FFT, 1 lag, 2 azimuth).
@@ -684,22 +685,23 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= e->device || e->device < 0)
         return bail(fail(DDM_ERR_NO_DEVICE, "no CUDA device " + std::to_string(e->device)));
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, e->device) != cudaSuccess || prop.major != 10)
+    // two attribute queries, not cudaGetDeviceProperties: that one was measured to take up to
+    // 0.3 s while the device is busy and to hold up other threads' launches meanwhile
+    int major = 0;
+    if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, e->device) != cudaSuccess || major != 10 ||
+        cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, e->device) != cudaSuccess)
         return bail(fail(DDM_ERR_NO_DEVICE, "device " + std::to_string(e->device) + " is not an sm_100 GPU"));
     if (cudaSetDevice(e->device) != cudaSuccess) return bail(fail(DDM_ERR_CUDA, "cudaSetDevice failed"));
-    e->sms = prop.multiProcessorCount;
     if (cfg->stream) {
         e->stream = static_cast<cudaStream_t>(cfg->stream);
     } else {
-        if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess)
-            return bail(fail(DDM_ERR_CUDA, "cudaStreamCreate failed"));
+        if (!(e->stream = stream_acquire(e->device))) return bail(fail(DDM_ERR_CUDA, "cudaStreamCreate failed"));
         e->own_stream = true;
     }
-    if (cudaStreamCreateWithFlags(&e->fft_stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&e->result_stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&e->upload_stream, cudaStreamNonBlocking) != cudaSuccess ||
+    // private streams from the process-wide pool (creating streams while the device is busy
+    // is slow and holds up other threads' launches)
+    if (!(e->fft_stream = stream_acquire(e->device)) || !(e->copy_stream = stream_acquire(e->device)) ||
+        !(e->result_stream = stream_acquire(e->device)) || !(e->upload_stream = stream_acquire(e->device)) ||
         cudaEventCreateWithFlags(&e->ev_isf_ready, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&e->ev_isf_read, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&e->ev_copy, cudaEventDisableTiming) != cudaSuccess ||

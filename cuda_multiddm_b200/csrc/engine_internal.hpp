@@ -11,6 +11,10 @@
 
 namespace ddm {
 
+// Private streams an engine takes from the stream pool (FFT, host copies, results, uploads)
+// when given a stream to queue on, as a server's engines are.
+constexpr int kEngineStreams = 4;
+
 struct DeferredLag {  // one lag launch an engine would have issued
     int J;
     const int *table;  // device copy of its table (the engine's table ring)

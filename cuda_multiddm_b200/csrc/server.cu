@@ -25,6 +25,7 @@
 #include "errors.hpp"
 #include "lag.cuh"
 #include "pinned_pool.hpp"
+#include "stream_pool.hpp"
 
 using namespace ddm;
 
@@ -66,6 +67,7 @@ struct Stream {
     long isf_size = 0;
     long chunks_submitted = 0, chunks_issued = 0, frames_issued = 0;
     LagMaps *maps_d = nullptr;
+    LagMaps *maps_h = nullptr;  // pinned source of the maps_d upload
     std::deque<PendingChunk> pending;
     std::vector<std::unique_ptr<Slot>> slots;
     std::deque<Slot *> order;  // slots in flight or ready, in chunk order
@@ -169,6 +171,7 @@ int pinned(PinnedBuf *b, size_t bytes) {
 void release_stream(Stream &st) {
     engine_close_async(st.eng);
     cudaFreeAsync(st.maps_d, nullptr);
+    pinned_release(st.maps_h);
     for (auto &sl : st.slots) {
         pinned_release(sl->isf_h);
         pinned_release(sl->status_h);
@@ -268,6 +271,9 @@ extern "C" int ddm_server_open(const ddm_server_config *cfg, ddm_server **out) {
         }
         cudaGetLastError();  // a budget the pool cannot map at once is not an error
     }
+    // the private streams of every slot's engine, made now while the device is idle (made
+    // while streams run, each took tens of milliseconds and held up the steps' launches)
+    StreamPool::get().reserve(s->device, kEngineStreams * s->max_streams);
     for (int i = 0; i < kItemRing; i++) CUDA_TRY(cudaEventCreateWithFlags(&s->items_ev[i], cudaEventDisableTiming));
     const int attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
 #define BATCH_ATTR(JJ) \
@@ -352,8 +358,13 @@ extern "C" int ddm_server_add_stream(ddm_server *s, const ddm_config *cfg, int *
     st.frame_bytes = static_cast<size_t>(cfg->frame_width) * cfg->frame_height * cfg->bytes_per_pixel;
     st.isf_size = ddm_isf_size(st.eng);
     const LagTarget t = engine_lag_target(st.eng);
-    bool ok = cudaMallocAsync(reinterpret_cast<void **>(&st.maps_d), sizeof(LagMaps), s->stream) == cudaSuccess &&
-              cudaMemcpyAsync(st.maps_d, t.maps, sizeof(LagMaps), cudaMemcpyHostToDevice, s->stream) == cudaSuccess;
+    // the tensor maps go up from page-locked memory: a copy from pageable memory may wait for
+    // the shared stream to drain, holding up this call and the steps' launches meanwhile
+    st.maps_h = static_cast<LagMaps *>(pinned_alloc(sizeof(LagMaps)));
+    bool ok = st.maps_h != nullptr;
+    if (ok) *st.maps_h = *t.maps;
+    ok = ok && cudaMallocAsync(reinterpret_cast<void **>(&st.maps_d), sizeof(LagMaps), s->stream) == cudaSuccess &&
+         cudaMemcpyAsync(st.maps_d, st.maps_h, sizeof(LagMaps), cudaMemcpyHostToDevice, s->stream) == cudaSuccess;
     for (int i = 0; ok && i < s->results_per_stream; i++) {
         auto sl = std::make_unique<Slot>();
         sl->server = s;
