@@ -41,7 +41,12 @@ class Config(C.Structure):
 
 class Info(C.Structure):
     _fields_ = [("frames_submitted", C.c_long), ("ring_slots", C.c_int), ("device_bytes", C.c_size_t),
-                ("kernel_launches", C.c_long), ("stream", C.c_void_p), ("frames_needed", C.c_long)]
+                ("kernel_launches", C.c_long), ("stream", C.c_void_p), ("frames_needed", C.c_long),
+                ("lag_batch_frames", C.c_int)]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("lag_batch_frames", C.c_int), ("frames_per_s", C.c_double), ("from_cache", C.c_int)]
 
 
 class ServerConfig(C.Structure):
@@ -73,6 +78,8 @@ SIGNATURES = {
     "ddm_isf_size": (C.c_long, [C.c_void_p]),
     "ddm_read_isf": (C.c_int, [C.c_void_p, C.c_void_p, C.c_long]),
     "ddm_finalize_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_long]),
+    "ddm_autotune": (C.c_int, [C.POINTER(Config), C.c_char_p, C.POINTER(Tuning)]),
+    "ddm_tune_key": (C.c_long, [C.POINTER(Config), C.c_char_p, C.c_long]),
     "ddm_wait_isf": (C.c_int, [C.c_void_p]),
     "ddm_dump_count": (C.c_int, [C.c_void_p]),
     "ddm_read_dump": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_long]),

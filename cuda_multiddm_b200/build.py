@@ -25,7 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC,-fopenmp,-ffp-contract=off",
               f"-I{ROOT / 'include'}", f"-I{CSRC}"]
 
-SOURCES = ["engine.cu", "server.cu", "noalloc.cu", "host.cpp", "synth.cpp", "movie.cpp"]
+SOURCES = ["engine.cu", "server.cu", "noalloc.cu", "host.cpp", "synth.cpp", "movie.cpp", "tune.cpp"]
 
 
 def _nvcc() -> str:

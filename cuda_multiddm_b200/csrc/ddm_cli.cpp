@@ -16,6 +16,8 @@
 //   -D UM_PER_PX         fit the ISF on the GPU (ddm_fit_isf) and write <out>fit
 //   -E compat|unbiased   estimator (default compat: the reference's own pairing)
 //   -P byte0|u16         16-bit pixel decoding (default byte0: the reference's first byte)
+//   -U CACHE             unbiased estimator: frames per lag launch from the autotuner
+//                        (ddm_autotune; timed once per shape and kept in the JSON file CACHE)
 #include <getopt.h>
 #include <unistd.h>
 
@@ -77,7 +79,9 @@ void print_help() {
                  "               write <PATH>fit with F, A, B per curve and the diffusion\n"
                  "               coefficient per tile and scale (UMPX: micrometres per pixel)\n"
                  "  -E MODE      compat (default) or unbiased estimator\n"
-                 "  -P MODE      byte0 (default) or u16 decoding of 16-bit pixels\n");
+                 "  -P MODE      byte0 (default) or u16 decoding of 16-bit pixels\n"
+                 "  -U CACHE     with -E unbiased: frames per lag launch picked by the autotuner,\n"
+                 "               timed once per shape and kept in the JSON file CACHE\n");
 }
 
 // Number text as std::ostream prints a float (6 significant digits), then one space, as
@@ -209,9 +213,10 @@ int main(int argc, char **argv) {
     double fit_um_per_px = 0.0;  // -D
     float tolerance = 1.2f;
     int estimator = DDM_EST_COMPAT, pixel_mode = DDM_PIX_BYTE0;
+    std::string tune_cache;  // -U
 
     for (;;) {
-        int c = getopt(argc, argv, "ho:N:s:x:y:Q:T:S:If:W::vZt:C:MG:F:B:K:AE:P:D:");
+        int c = getopt(argc, argv, "ho:N:s:x:y:Q:T:S:If:W::vZt:C:MG:F:B:K:AE:P:D:U:");
         if (c == -1) break;
         switch (c) {
             case '?':
@@ -250,6 +255,7 @@ int main(int argc, char **argv) {
                 else if (!std::strcmp(optarg, "unbiased")) estimator = DDM_EST_UNBIASED;
                 else die("-E takes compat or unbiased");
                 break;
+            case 'U': tune_cache = optarg; break;
             case 'P':
                 if (!std::strcmp(optarg, "byte0")) pixel_mode = DDM_PIX_BYTE0;
                 else if (!std::strcmp(optarg, "u16")) pixel_mode = DDM_PIX_U16LE;
@@ -341,6 +347,15 @@ int main(int argc, char **argv) {
     cfg.multistream = multistream ? 1 : 0;
     cfg.total_frames = frame_count;
     cfg.dump_every = rolling;
+    if (!tune_cache.empty()) {
+        if (estimator != DDM_EST_UNBIASED) die("-U tunes the unbiased estimator (-E unbiased)");
+        ddm_tuning tuned;
+        if (ddm_autotune(&cfg, tune_cache.c_str(), &tuned) != DDM_OK) die(ddm_last_error());
+        cfg.lag_batch_frames = tuned.lag_batch_frames;
+        if (g_verbose)
+            std::fprintf(stderr, "[Info] lag_batch_frames %d (%s)\n", tuned.lag_batch_frames,
+                         tuned.from_cache ? "cached" : "timed");
+    }
     ddm_engine *eng = nullptr;
     if (ddm_open(&cfg, &eng) != DDM_OK) die(ddm_last_error());
     ddm_info info;

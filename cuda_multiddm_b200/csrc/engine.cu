@@ -12,6 +12,7 @@
 //   masks  int    CSR of annulus element indices per (scale, q); counts [S][Q].
 //   isf    double [sum_s tiles_s * Q * T].
 #include <algorithm>
+#include <cstdlib>
 #include <functional>
 #include <cmath>
 #include <cstdio>
@@ -31,6 +32,7 @@
 #include "lag_host.hpp"
 #include "pinned_pool.hpp"
 #include "stream_pool.hpp"
+#include "tune.hpp"
 
 namespace ddm {
 
@@ -641,12 +643,17 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
 
     // Schedule and ring size
     e->jmax = std::min(kPieceFrames, e->C);
-    if (cfg->lag_batch_frames < 0 || cfg->lag_batch_frames > kMaxJ)
-        return bail(fail(DDM_ERR_INVALID_ARG, "lag_batch_frames must be 0.." + std::to_string(kMaxJ)));
+    if (cfg->lag_batch_frames < -1 || cfg->lag_batch_frames > kMaxJ)
+        return bail(fail(DDM_ERR_INVALID_ARG, "lag_batch_frames must be -1.." + std::to_string(kMaxJ)));
+    int lag_batch_cfg = cfg->lag_batch_frames;
+    if (lag_batch_cfg == -1) {  // the tuned value for this shape, if a cache names one
+        int tuned = 0;
+        lag_batch_cfg = tune_lookup(std::getenv("DDM_TUNE_CACHE"), tune_key(cfg), &tuned, nullptr) ? tuned : 0;
+    }
     // default: unbiased launches of kPieceFrames (32) frames, the instantiated register-frame
     // count the kernel's cost per launch is set by (32 frames take about the time of 30);
     // compat iterations in blocks of one ingest piece
-    e->lag_batch = cfg->lag_batch_frames ? cfg->lag_batch_frames : (compat ? e->jmax : kPieceFrames);
+    e->lag_batch = lag_batch_cfg ? lag_batch_cfg : (compat ? e->jmax : kPieceFrames);
     if (compat) {
         e->its = compat_schedule(e->N, e->C, e->multistream, e->G, e->taus, &e->frames_read);
         // Frames arrive in pieces of jmax and iterations run in order, each once every
@@ -1211,6 +1218,7 @@ extern "C" int ddm_get_info(const ddm_engine *e, ddm_info *info) {
     info->kernel_launches = static_cast<long>(e->launches);
     info->stream = e->stream;
     info->frames_needed = e->estimator == DDM_EST_COMPAT ? e->frames_read : 0;
+    info->lag_batch_frames = e->lag_batch;
     return DDM_OK;
 }
 

@@ -33,7 +33,8 @@ class EngineConfig:
     hbm_budget_bytes: int = 0
     device: int = 0
     stream: int | None = None          # a cudaStream_t as an integer, or None
-    lag_batch_frames: int = 0          # frames per lag launch (1..64; 0 = 32 unbiased, min(chunk_frames, 32) compat)
+    lag_batch_frames: int = 0          # frames per lag launch (1..64; 0 = 32 unbiased, min(chunk_frames, 32) compat;
+                                       # -1 = the value autotune() cached for this shape in $DDM_TUNE_CACHE)
     _keep: list = field(default_factory=list, repr=False)
 
     def to_c(self) -> Config:
@@ -48,6 +49,27 @@ class EngineConfig:
                       C.c_float(self.tolerance), self.chunk_frames, est, int(bool(self.multistream)),
                       self.total_frames, self.dump_every, self.hbm_budget_bytes, self.device,
                       C.c_void_p(self.stream) if self.stream else None, self.lag_batch_frames)
+
+
+def tune_key(cfg: EngineConfig) -> str:
+    """The shape key the autotuner's cache files results under."""
+    c = cfg.to_c()
+    n = lib().ddm_tune_key(C.byref(c), None, 0)
+    buf = C.create_string_buffer(n + 1)
+    lib().ddm_tune_key(C.byref(c), buf, n + 1)
+    return buf.value.decode()
+
+
+def autotune(cfg: EngineConfig, cache: str | None = None) -> dict:
+    """Time lag_batch_frames candidates on cfg's shape (unbiased estimator) and return
+    {"lag_batch_frames", "frames_per_s", "from_cache"}; with `cache`, look the shape up there
+    first and store the result afterwards (engines opened with lag_batch_frames = -1 and
+    DDM_TUNE_CACHE set to that file use it)."""
+    from ._lib import Tuning
+    c = cfg.to_c()
+    t = Tuning()
+    check(lib().ddm_autotune(C.byref(c), cache.encode() if cache else None, C.byref(t)))
+    return {"lag_batch_frames": t.lag_batch_frames, "frames_per_s": t.frames_per_s, "from_cache": bool(t.from_cache)}
 
 
 def isf_blocks(isf: np.ndarray, scales: Sequence[int], n_lambda: int, n_tau: int) -> dict:

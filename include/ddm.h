@@ -78,7 +78,9 @@ typedef struct {
                                       up to lag_batch_frames - 1 frames may wait in the ring
                                       for a fuller launch (fuller launches read fewer partner
                                       bytes per frame); finalize/synchronize pair them. Compat
-                                      (0 = min(C, 32)): A-frames per launch. */
+                                      (0 = min(C, 32)): A-frames per launch. -1: the value
+                                      ddm_autotune cached for this shape in the file named by
+                                      the DDM_TUNE_CACHE environment variable, else as 0. */
 } ddm_config;
 
 typedef struct ddm_engine ddm_engine;
@@ -131,6 +133,22 @@ int ddm_finalize_async(ddm_engine *e, double *isf_out, long capacity);
 /* Block until the last ddm_finalize_async result is in its buffer; returns DDM_ERR_CUDA if
  * a kernel queued before it reported a failure (the status ddm_finalize checks). */
 int ddm_wait_isf(ddm_engine *e);
+
+/* Lag-blocking autotuner (the reference has none; its work is one launch per (scale, tau,
+ * frame)). ddm_autotune times lag_batch_frames = 16, 24, 30, 32, 64 and the chunk size on
+ * cfg's shape (unbiased estimator only) with synthetic frames on the device, in the engine's
+ * steady state, and returns the fastest; with a cache path it first looks the shape up
+ * there and afterwards stores the result (a JSON object, one shape key per line, with the
+ * frames/s of every candidate). ddm_tune_key writes the shape key (frame size and depth,
+ * scales, tau count / largest / hash, chunk, estimator) into out (capacity bytes, NUL
+ * terminated) and returns its length, or -1. */
+typedef struct {
+    int lag_batch_frames;
+    double frames_per_s;   /* of the winner, as timed (or as cached) */
+    int from_cache;        /* 1: found in the cache, nothing timed */
+} ddm_tuning;
+int ddm_autotune(const ddm_config *cfg, const char *cache_path, ddm_tuning *out);
+long ddm_tune_key(const ddm_config *cfg, char *out, long capacity);
 
 /* -G snapshots (src/DDM.cu:800-826): number of snapshots taken so far, and a copy of
  * snapshot `index` in the ddm_read_isf layout. */
@@ -210,6 +228,7 @@ typedef struct {
     long kernel_launches;
     void *stream;
     long frames_needed;
+    int lag_batch_frames;          /* frames per lag launch in use (after defaults / tuning) */
 } ddm_info;
 int ddm_get_info(const ddm_engine *e, ddm_info *info);
 
