@@ -310,10 +310,13 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
         col_ctas += fs.ctas_per_frame;
         smem = std::max(smem, fft_smem_bytes(s));
     }
-    // Frames go through both passes in groups small enough for the row pass's output to
-    // stay in L2 until the column pass reads it.
+    // Frames go through both passes in groups of up to 256 MB of spectra (15 frames of the
+    // 1024^2 x 4-scale shape): fewer, larger launches were measured faster than groups small
+    // enough for the row pass's output to stay in L2 (frames/s at 34 / 64 / 100 / 256 MB:
+    // 0.98 / 1 / 1.015 / 1.025), and two or more groups per piece keep the host copies of a
+    // group overlapping the FFT of the one before (one group per piece: -6 % end to end).
     const long long frame_bytes = e->E * static_cast<long long>(sizeof(float2));
-    const int group = static_cast<int>(std::max<long long>(1, std::min<long long>(nframes, (64LL << 20) / frame_bytes)));
+    const int group = static_cast<int>(std::max<long long>(1, std::min<long long>(nframes, (256LL << 20) / frame_bytes)));
     for (int f0 = 0; f0 < nframes; f0 += group) {
         const int nf = std::min(group, nframes - f0);
         if (before_group) {
