@@ -9,7 +9,7 @@ For each case in cases.py it writes the synthetic video as an IIDC .movie file p
 lambda / tau / scale files, runs the reference CLI on it, and stores every ISF text file it
 writes; it also records buildAzimuthMask counts and mask hashes, and analyseFFTDevice
 outputs, from ref_harness. Output: OUTDIR/reference_outputs.json (default
-gpurun_out/golden), copied by hand into tests/golden/.
+tests/golden/_out), copied by hand into tests/golden/.
 """
 from __future__ import annotations
 
@@ -77,7 +77,7 @@ def run_reduce() -> list:
 
 
 def main() -> None:
-    outdir = Path(sys.argv[1]) if len(sys.argv) > 1 else ROOT / "gpurun_out" / "golden"
+    outdir = Path(sys.argv[1]) if len(sys.argv) > 1 else ROOT / "tests" / "golden" / "_out"
     outdir.mkdir(parents=True, exist_ok=True)
     result = {"reference": "zhangyuyi99/cuda_multiDDM src/, built by oracle/Makefile for sm_100a",
               "cases": [], "masks": run_masks(), "reduce": run_reduce()}
