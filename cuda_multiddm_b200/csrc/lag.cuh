@@ -180,11 +180,12 @@ struct LagMaps {
 // Warp-specialised pipeline over groups of kLagGroup union entries. A run of kLagFuse
 // entries (table flag kLagRunFlag) is one pass over the span of its windows. Warps
 // 0..kLagConsumerWarps-1 consume; the last warp produces (its lane 0 issues the copies).
-// Group g occupies shared-memory slots [(g % kGS) * kLagGroup, +kLagGroup) with
-// kGS = lag_group_slots(J); its consecutive ring slots arrive as a few 2-D boxes (runs) that
-// all complete on full[g % kGS]; empty[g % kGS] completes when every consumer warp has moved
-// past the group. Union entry u of the CTA's n-th element block (n = 0, 1, ...) therefore
-// sits in shared-memory slot (n * ngroups * kLagGroup + u) % lag_ring_slots(J). Neither side
+// Running group G (group g of the CTA's n-th element block, G = n * ngroups + g) occupies
+// shared-memory slots [(G % kGS) * kLagGroup, +kLagGroup) with kGS = lag_group_slots(J); its
+// consecutive ring slots arrive as a few 2-D boxes (runs) that all complete on full[G % kGS];
+// empty[G % kGS] completes when every consumer warp has moved past the group. Union entry u
+// of the n-th element block therefore sits in shared-memory slot
+// (n * ngroups * kLagGroup + u) % lag_ring_slots(J). Neither side
 // ever waits for the whole CTA. The CTA handles element blocks block_begin, + block_step, ...
 // below block_end; `maps` may live in kernel parameter space or global memory.
 template <int J>
