@@ -200,6 +200,18 @@ def test_fused_tau_runs_match_oracle():
         assert_isf_close(isf, want, scales, len(lambdas), len(taus))
 
 
+def test_fused_runs_over_many_element_blocks_match_oracle():
+    """Fused tau runs with every CTA of the persistent lag grid walking several element blocks
+    (512^2 frames, three scales: about 3,100 blocks of 128 elements for 444 CTAs, so the group
+    counter runs on across blocks), in 32-frame and 64-frame (two-lane) launches."""
+    frames = media.synth_video(49, 512, 512, 70, 1000, step_var=1.0)
+    scales, taus, lambdas = [512, 256, 128], list(range(1, 14)) + [20, 31], [3.0, 6.0, 12.0, 24.0, 48.0]
+    want, _ = O.ddm_run(frames, scales, taus, lambdas, estimator=O.EST_UNBIASED, chunk=10)
+    for lb in (32, 64):
+        isf, _, _ = engine_run(frames, scales, taus, lambdas, estimator="unbiased", C=10, lag_batch=lb)
+        assert_isf_close(isf, want, scales, len(lambdas), len(taus))
+
+
 def test_finalize_async_matches_finalize():
     """A live result per chunk through ddm_finalize_async, the next chunk submitted while the
     result is on its way, equals ddm_finalize + ddm_read_isf after every chunk bit for bit
