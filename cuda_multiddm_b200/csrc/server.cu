@@ -32,6 +32,7 @@ using namespace ddm;
 namespace {
 
 constexpr int kItemRing = 4;  // batch descriptor buffers in flight
+constexpr size_t kPinnedArenaBytes = 2ull << 30;  // page-locked at server open for the pinned pool's misses
 
 using Clock = std::chrono::steady_clock;
 
@@ -274,6 +275,9 @@ extern "C" int ddm_server_open(const ddm_server_config *cfg, ddm_server **out) {
     // the private streams of every slot's engine, made now while the device is idle (made
     // while streams run, each took tens of milliseconds and held up the steps' launches)
     StreamPool::get().reserve(s->device, kEngineStreams * s->max_streams);
+    // and page-locked memory for the streams' chunk and result buffers (a miss of the pinned
+    // pool otherwise pins memory while the admitted streams run); not an error if refused
+    if (!PinnedPool::get().reserve_arena(kPinnedArenaBytes)) cudaGetLastError();
     for (int i = 0; i < kItemRing; i++) CUDA_TRY(cudaEventCreateWithFlags(&s->items_ev[i], cudaEventDisableTiming));
     const int attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
 #define BATCH_ATTR(JJ) \
