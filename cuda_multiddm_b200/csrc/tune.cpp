@@ -200,14 +200,15 @@ extern "C" int ddm_autotune(const ddm_config *cfg, const char *cache_path, ddm_t
     cands.erase(std::unique(cands.begin(), cands.end()), cands.end());
     const int timed = std::max(4, (8 * 30 + cfg->chunk_frames - 1) / cfg->chunk_frames);
     std::ostringstream tried;
-    int best = 0;
+    int best = 0, first_error = DDM_OK;
+    std::string first_message;
     double best_fps = 0.0;
-    for (int J : cands) {
+    for (int J : cands) {  // a candidate that cannot run here (e.g. its ring does not fit) is skipped
         double fps = 0.0;
         const int st = time_candidate(*cfg, J, dev, n_frames, timed, &fps);
         if (st) {
-            cudaFree(dev);
-            return st;
+            if (!first_error) first_error = st, first_message = last_error();
+            continue;
         }
         char buf[64];
         std::snprintf(buf, sizeof(buf), "%s\"%d\": %.1f", tried.tellp() > 0 ? ", " : "", J, fps);
@@ -215,6 +216,7 @@ extern "C" int ddm_autotune(const ddm_config *cfg, const char *cache_path, ddm_t
         if (fps > best_fps) best_fps = fps, best = J;
     }
     cudaFree(dev);
+    if (best == 0) return fail(first_error ? first_error : DDM_ERR_CUDA, "ddm_autotune: no candidate ran: " + first_message);
     out->lag_batch_frames = best;
     out->frames_per_s = best_fps;
     out->from_cache = 0;
