@@ -341,6 +341,10 @@ typedef struct {
                                operation to its last (queueing excluded) */
 } ddm_server_stats;
 
+/* Opens a server on cfg->device. At open it maps its HBM budget into the device's memory pool,
+ * creates the private CUDA streams of every stream slot (4 each) and page-locks a 2 GiB host
+ * arena for the streams' chunk and result buffers (once per process; skipped if refused), so
+ * that admitting a stream later touches none of these slow driver paths. */
 int ddm_server_open(const ddm_server_config *cfg, ddm_server **out);
 int ddm_server_close(ddm_server *s);
 /* Admit a stream (cfg as for ddm_open; its device, stream, lag_batch_frames and dump_every
