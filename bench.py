@@ -1,28 +1,41 @@
 """Benchmark of the multi-scale DDM hot path on B200.
 
-Workload (the multi-scale FP32 configuration): 1000 frames of 1024x1024 uint8 synthetic
-Brownian-particle video (4000 Gaussian spots, sigma 2 px, amplitude 120 on background 20,
-steps N(0, 2 px^2) per axis per frame, i.e. D = 1 px^2/frame, Gaussian noise sd 4),
-scales {1024, 512, 256, 128}, 64 taus log-spaced 1..500, 30 lambdas log-spaced 2..512 px,
-tolerance 1.2, chunks of 30 frames, unbiased estimator (tau_max > chunk).
+Workloads (seeded synthetic Brownian-particle video; the reference ships no data):
+
+  c2 (default, the headline)  1000 frames of 1024x1024 uint8 (4000 Gaussian spots, sigma 2 px,
+      amplitude 120 on background 20, steps N(0, 2 px^2) per axis per frame, i.e.
+      D = 1 px^2/frame, Gaussian noise sd 4), scales {1024, 512, 256, 128}, 64 taus
+      log-spaced 1..500, 30 lambdas log-spaced 2..512 px, tolerance 1.2, 30-frame chunks,
+      unbiased estimator (tau_max > chunk)
+  c1  200 frames of 256^2 uint8 (300 spots, steps N(0, 0.5 px^2)), one 256 tile, taus 1..20,
+      10 lambdas log 4..128
+  c3  600 frames of 2048^2 uint8 (16000 spots, D = 0.5), scales 2048..32 (5461 tiles per
+      frame), 48 taus log 1..300, 40 lambdas log 2..1024
+  c4  800 frames of 2048^2 uint16 holding 12-bit values (spots of amplitude 2000 on 300,
+      Poisson shot noise, half the spots with D = 0.2 and half with D = 2.0), scales
+      {2048, 1024, 512, 256}, 64 taus log 1..400, 30 lambdas log 2..1024, full 16-bit decode
+  small  c2's taus and chunk on 512^2 frames (profiling captures only)
+  serving  many camera streams through one server (its own JSON line)
 
 One step = one chunk of 30 frames through the engine: extraction + 2-D R2C FFT of every
-tile at every scale into the device ring, then |F(t) - F(t-tau)|^2 for all 64 taus of the
+tile at every scale into the device ring, then |F(t) - F(t-tau)|^2 for every tau of the
 30 new frames. The ring is pre-filled with ceil(tau_max / chunk) + 1 chunks first, so every
-timed frame pairs at all 64 lags (steady state). The video is 1000 frames long and the
-steps cycle through it. The timed region ends with the azimuthal average (ISF ready).
+timed frame pairs at every lag (steady state). The steps cycle through the video. The
+timed region ends with the azimuthal average (ISF ready).
 
   value    frames/s with the video resident in HBM (device pointers submitted)
   e2e      frames/s through the public API from pinned host memory: every step copies its
            30 frames host->device and reads the updated ISF (a live result) device->host
-  roofline the lag kernel against HBM, with the algorithmic bytes per analysed frame
-           8*E*(T+1) + 16*T*E/C (one F(t) read, one F(t-tau) read per tau, Kahan
-           accumulators read+written once per chunk), E = 2,112,512 complex per frame;
-           the kernel reads each distinct partner frame of a launch once (0.30 of those
-           bytes), so frac is above 1, and traffic / traffic_gbs / traffic_frac give the
-           ncu-measured DRAM bytes per launch and their rate over the same launch time
+  roofline the lag kernel against HBM: achieved = the compulsory DRAM bytes of its launches
+           (each register frame and each distinct partner frame of a launch read once, each
+           accumulator row read and written once; counted by the engine) / their CUDA-event
+           time. model_frac gives the same launches against the survey's byte model
+           8*E*(T+1) + 16*T*E/C per frame (one partner read per (frame, tau)), which the
+           kernel beats by reusing partners, so it is above 1; traffic is ncu-measured DRAM
+           bytes where a capture exists (traffic_source says which)
 
-  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+  python bench.py [--workload c1|c2|c3|c4|small|serving] [--gpus N --steps K --warmup W]
+                  [--impl reference]
 """
 from __future__ import annotations
 
@@ -41,36 +54,86 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "frames/s analysed (1024^2, 4 scales, 64 tau)"
 UNIT = "frames/s"
-SCALES = [1024, 512, 256, 128]
 CHUNK = 30
-N_FRAMES = 1000
-SIDE = 1024
-# A 4x smaller frame with the same tau list and chunk (the same lag schedule per element),
-# small enough for ncu captures that save and restore device memory (about 3 GB held).
-SMALL = dict(SIDE=512, SCALES=[512, 256, 128, 64], N_FRAMES=300)
 
 
-def workload():
-    from cuda_multiddm_b200.media import log_lambdas, log_taus
-    return log_taus(1, 500, 64), log_lambdas(2, 512, 30)
+def log_taus(lo: int, hi: int, n: int) -> list[int]:
+    """n strictly increasing lags from lo to hi, log-spaced (cuda_multiddm_b200.media.log_taus;
+    restated here so that the reference arm imports nothing of the product)."""
+    out: list[int] = []
+    for i in range(n):
+        v = int(round(lo * (hi / lo) ** (i / (n - 1)))) if n > 1 else lo
+        if out and v <= out[-1]:
+            v = out[-1] + 1
+        out.append(v)
+    return out
 
 
-def frames_elements() -> int:
-    return sum((SIDE // s) ** 2 * s * (s // 2 + 1) for s in SCALES)
+def log_lambdas(lo: float, hi: float, n: int) -> list[float]:
+    """n log-spaced wavelengths rounded to float32 (cuda_multiddm_b200.media.log_lambdas)."""
+    return [float(np.float32(lo * (hi / lo) ** (i / (n - 1)))) if n > 1 else float(np.float32(lo))
+            for i in range(n)]
 
 
-def lag_bytes_per_frame(T: int) -> float:
-    E = frames_elements()
+# name -> workload. video: synth_video keyword arguments; spots scale with the frame area.
+WORKLOADS = {
+    "c1": dict(workload="plain_256_1scale_20tau", side=256, frames=200, scales=[256],
+               taus=list(range(1, 21)), lambdas=log_lambdas(4, 128, 10), pixel_mode="byte0",
+               video=dict(spots=300, step_var=0.5)),
+    "c2": dict(workload="multiscale_1024_4scales_64tau", side=1024, frames=1000, scales=[1024, 512, 256, 128],
+               taus=log_taus(1, 500, 64), lambdas=log_lambdas(2, 512, 30), pixel_mode="byte0",
+               video=dict(spots=4000, step_var=2.0)),
+    "c3": dict(workload="fine_2048_7scales_48tau", side=2048, frames=600,
+               scales=[2048, 1024, 512, 256, 128, 64, 32], taus=log_taus(1, 300, 48),
+               lambdas=log_lambdas(2, 1024, 40), pixel_mode="byte0", video=dict(spots=16000, step_var=1.0)),
+    "c4": dict(workload="highbit_2048_u16_4scales_64tau", side=2048, frames=800, scales=[2048, 1024, 512, 256],
+               taus=log_taus(1, 400, 64), lambdas=log_lambdas(2, 1024, 30), pixel_mode="u16",
+               video=dict(spots=16000, amplitude=2000.0, background=300.0, noise_sd=-1.0, max_value=4095,
+                          step_var=0.4, step_var_b=4.0)),
+    "small": dict(workload="small_512_4scales_64tau (profiling)", side=512, frames=300, scales=[512, 256, 128, 64],
+                  taus=log_taus(1, 500, 64), lambdas=log_lambdas(2, 512, 30), pixel_mode="byte0",
+                  video=dict(spots=1000, step_var=2.0)),
+}
+WORKLOADS["multiscale"] = WORKLOADS["c2"]
+
+
+def metric(w: dict) -> str:
+    if w is WORKLOADS["c2"]:
+        return "frames/s analysed (1024^2, 4 scales, 64 tau)"
+    return f"frames/s analysed ({w['side']}^2, {len(w['scales'])} scales, {len(w['taus'])} tau)"
+
+
+def frames_elements(w: dict) -> int:
+    M = w["side"]
+    return sum((M // s) ** 2 * s * (s // 2 + 1) for s in w["scales"])
+
+
+def bytes_per_pixel(w: dict) -> int:
+    return 2 if w["video"].get("max_value", 255) > 255 else 1
+
+
+def model_bytes_per_frame(w: dict) -> float:
+    """The survey's lag-kernel byte model: one F(t) read, one F(t - tau) read per tau, and the
+    accumulators read and written once per 30-frame chunk."""
+    E, T = frames_elements(w), len(w["taus"])
     return 8.0 * E * (T + 1) + 16.0 * T * E / CHUNK
 
 
-def make_video(seed: int, frames: int | None = None) -> np.ndarray:
-    from cuda_multiddm_b200.media import synth_video
-    spots = 4000 * SIDE * SIDE // (1024 * 1024)  # same spot density at every frame size
-    return synth_video(seed, SIDE, SIDE, N_FRAMES if frames is None else frames, spots, spot_sigma=2.0,
-                       amplitude=120.0, background=20.0, step_var=2.0, noise_sd=4.0, max_value=255)
+def video_kwargs(w: dict) -> dict:
+    kw = dict(spot_sigma=2.0, amplitude=120.0, background=20.0, noise_sd=4.0, max_value=255)
+    kw.update(w["video"])
+    return kw
+
+
+def config_of(w: dict, world: int) -> dict:
+    """The workload as both arms report it (identical keys and values)."""
+    return {"workload": w["workload"], "frames": w["frames"], "side": w["side"], "scales": w["scales"],
+            "taus": len(w["taus"]), "tau_max": max(w["taus"]), "lambdas": len(w["lambdas"]), "tolerance": 1.2,
+            "chunk": CHUNK, "estimator": "unbiased", "pixel": "u16 (12-bit values)" if bytes_per_pixel(w) == 2
+            else "u8", "steady_state": True,
+            "l2": "inputs larger than L2: every step streams a ring of spectra far larger than 126 MB",
+            "parallelism": f"replicas x{world} (independent streams, no collective)"}
 
 
 def measured_peaks():
@@ -81,19 +144,24 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(frames_per_launch: float):
-    """DRAM bytes per lag launch of `frames_per_launch` frames, from the per-frame DRAM
-    traffic in the committed ncu summary of the lag kernel (None if absent)."""
+def profiled_traffic(w: dict, frames: float):
+    """ncu DRAM bytes of the lag kernel for `frames` analysed frames, from the per-frame
+    figure in the committed capture of the headline workload (None for other workloads)."""
+    if w is not WORKLOADS["c2"]:
+        return None, None
     p = ROOT / "profiles" / "lag_kernel_c2.txt"
     if not p.exists():
-        return None
+        return None, None
+    src = None
     for line in p.read_text().splitlines():
+        if line.startswith("traffic_source:"):
+            src = line.split(":", 1)[1].strip()
         if line.startswith("traffic_bytes_per_frame:"):
             try:
-                return float(line.split(":", 1)[1].split()[0]) * frames_per_launch
+                return float(line.split(":", 1)[1].split()[0]) * frames, src
             except ValueError:
-                return None
-    return None
+                return None, None
+    return None, None
 
 
 class ClockSampler:
@@ -144,54 +212,89 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_baseline(seconds_hint: float = 20.0) -> dict:
-    """The FP64 oracle (a port of the reference's path; the reference has no CPU path)
-    timed on this host's cores, in steady state, on a bounded sample of frames."""
+# ------------------------------------------------------------------------------------------
+# CPU side: the FP64 oracle (a port of the reference's algorithm; the reference has no CPU
+# path). Its input comes from the oracle's own restatement of the generator, so this side
+# never loads the product library.
+# ------------------------------------------------------------------------------------------
+
+def oracle_video(w: dict, seed: int):
     from oracle import oracle as O
-    taus, _ = workload()
-    video = make_video(1002, frames=8)
+    return O.synth_video(seed, w["side"], w["side"], w["frames"], **video_kwargs(w))
+
+
+def oracle_seconds(video, w: dict, warm: int, timed: int, threads: int) -> float:
+    from oracle import oracle as O
+    pix = O.PIX_U16LE if w["pixel_mode"] == "u16" else O.PIX_BYTE0
+    return O.bench_steady(video, w["scales"], w["taus"], timed, threads, warm_frames=warm, pixmode=pix)
+
+
+def cpu_sample(w: dict, video, seconds: float, threads: int) -> tuple[int, float, float]:
+    """(frames, seconds, seconds of one frame): a steady-state oracle sample of about
+    `seconds` of timed work after one untimed frame."""
+    t1 = oracle_seconds(video, w, 1, 1, threads)
+    n = max(1, min(256, int(seconds / max(t1, 1e-4))))
+    t = oracle_seconds(video, w, 1, n, threads) if n > 1 else t1
+    return n, t, t1
+
+
+def cpu_baseline(w: dict, seed: int) -> dict:
     threads = os.cpu_count() or 1
-    # one timed frame first, then as many as fit the hint
-    t1 = O.bench_steady(video, SCALES, taus, 1, threads)
-    n = max(1, min(64, int(seconds_hint / max(t1, 1e-3))))
-    t = O.bench_steady(video, SCALES, taus, n, threads) if n > 1 else t1
+    video = oracle_video(w, seed)
+    try:
+        n, t, _ = cpu_sample(w, video, 20.0, threads)
+    except MemoryError as exc:
+        return {"value": None, "unit": UNIT, "cores": threads, "kind": "port", "sample": f"unavailable: {exc}"}
     return {"value": n / t, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{n} steady-state frames of the 1024^2 x 4-scale x 64-tau workload, FP64 oracle "
-                      f"(extract + R2C FFT at every scale + 64 lag pairs per frame), OpenMP {threads} threads"}
+            "sample": f"{n} steady-state frames of the {w['workload']} workload after one untimed frame, FP64 "
+                      f"oracle (extract + R2C FFT at every scale + {len(w['taus'])} lag pairs per frame), "
+                      f"OpenMP {threads} threads"}
 
 
-def job_throughput(times_ms, frames_per_rank: int, world: int, device=None):
-    """Whole-job throughput of `world` ranks that each analysed frames_per_rank frames:
-    every timing is reduced to its maximum over ranks (the job ends when the slowest rank
-    does). Returns (value, e2e_value, max_ms, max_e2e_ms) for times_ms = [device, e2e]."""
-    import torch
-    t = torch.tensor(times_ms, dtype=torch.float64, device=device)
-    if world > 1:
-        import torch.distributed as dist
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total = frames_per_rank * world
-    return total / (float(t[0]) / 1000.0), total / (float(t[1]) / 1000.0), float(t[0]), float(t[1])
-
-
-def run_reference(args) -> None:
+def run_reference(args, w: dict) -> None:
+    """The reference arm: the FP64 oracle port of the reference's algorithm on the host cores
+    (the reference has no CPU implementation of this path, and its CUDA build reads past its
+    accumulator on multi-tile scales with several taus). Rank 0 alone runs. Each step is a
+    sample of `f` frames of the workload (30, the chunk, when the whole run fits a few
+    minutes; fewer for the larger workloads); W warm-up steps run untimed, then K steps are
+    timed as one stretch, and ms_per_step is that stretch / K."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    base = cpu_baseline(seconds_hint=max(5.0, 2.0 * args.steps))
-    line = {"metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 * CHUNK / base["value"], "higher_is_better": True,
+    threads = os.cpu_count() or 1
+    video = oracle_video(w, 1002)
+    t1 = oracle_seconds(video, w, 1, 1, threads)
+    budget = 150.0  # seconds of oracle work for warm-up + timed steps
+    f = max(1, min(CHUNK, int(budget / max(t1, 1e-4) / (args.steps + args.warmup))))
+    secs = oracle_seconds(video, w, args.warmup * f, args.steps * f, threads)
+    value = args.steps * f / secs
+    sample = (f"each step: {f} steady-state frames of the {w['workload']} workload ({args.warmup} untimed "
+              f"warm-up steps first), FP64 oracle (extract + R2C FFT at every scale + {len(w['taus'])} lag pairs "
+              f"per frame), OpenMP {threads} threads")
+    line = {"metric": metric(w), "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * secs / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "multiscale_1024_4scales_64tau", "frames": N_FRAMES, "side": SIDE,
-                       "scales": SCALES, "taus": 64, "lambdas": 30, "chunk": CHUNK},
-            "impl": "reference", "cpu_baseline": base,
-            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "config": config_of(w, world), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "frames_per_step": f,
             "note": "the reference has no CPU implementation of this path; its GPU build cannot run this "
                     "configuration without reading past its accumulator allocation, so the reference arm "
                     "is the FP64 oracle port of its algorithm on the host cores"}
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args) -> None:
+# ------------------------------------------------------------------------------------------
+# GPU side
+# ------------------------------------------------------------------------------------------
+
+def make_video(w: dict, seed: int) -> np.ndarray:
+    from cuda_multiddm_b200.media import synth_video
+    return synth_video(seed, w["side"], w["side"], w["frames"], **video_kwargs(w))
+
+
+def run_ours(args, w: dict) -> None:
     import torch
     import torch.distributed as dist
 
@@ -206,14 +309,16 @@ def run_ours(args) -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
 
-    taus, lambdas = workload()
+    taus, lambdas, side, nfr = w["taus"], w["lambdas"], w["side"], w["frames"]
     T = len(taus)
-    video = make_video(1002 + rank)
-    dev_video = torch.from_numpy(video).cuda()
-    host_video = torch.from_numpy(video).pin_memory()
-    cfg = EngineConfig(frame_width=SIDE, frame_height=SIDE, scales=SCALES, taus=taus, lambdas=lambdas,
+    bpp = bytes_per_pixel(w)
+    video = make_video(w, 1002 + rank)
+    raw = video.view(np.uint8).reshape(nfr, side, side * bpp)
+    dev_video = torch.from_numpy(raw).cuda()
+    host_video = torch.from_numpy(raw).pin_memory()
+    cfg = EngineConfig(frame_width=side, frame_height=side, scales=w["scales"], taus=taus, lambdas=lambdas,
                        tolerance=1.2, chunk_frames=CHUNK, estimator="unbiased", device=local,
-                       lag_batch_frames=args.lag_batch)
+                       lag_batch_frames=args.lag_batch, bytes_per_pixel=bpp, pixel_mode=w["pixel_mode"])
     eng = Engine(cfg)
     stream = torch.cuda.ExternalStream(eng.info().stream)
     preroll = math.ceil(max(taus) / CHUNK) + 1
@@ -221,7 +326,7 @@ def run_ours(args) -> None:
 
     def next_chunk():
         i = cursor[0]
-        cursor[0] = (i + CHUNK) % (N_FRAMES - N_FRAMES % CHUNK)
+        cursor[0] = (i + CHUNK) % (nfr - nfr % CHUNK)
         return i
 
     def step_device():
@@ -235,7 +340,7 @@ def run_ours(args) -> None:
 
     # ---- device-resident timed region --------------------------------------------
     eng.set_timing(True)
-    eng.kernel_times()  # clear
+    eng.kernel_stats()  # clear
     launches0 = eng.info().kernel_launches
     sampler = ClockSampler(local)
     sampler.start()
@@ -252,7 +357,7 @@ def run_ours(args) -> None:
     torch.cuda.synchronize()
     clocks = sampler.stop()
     elapsed_ms = ev0.elapsed_time(ev1)
-    ktimes = eng.kernel_times()
+    kstats = eng.kernel_stats()
     launches = eng.info().kernel_launches - launches0
     if world > 1:
         dist.barrier()
@@ -292,51 +397,63 @@ def run_ours(args) -> None:
     value, e2e_value, elapsed_ms, e2e_ms = job_throughput(
         [elapsed_ms, e2e_ms], args.steps * CHUNK, world, "cuda" if world > 1 else None)
 
-    # Lag launches pair up to --lag-batch frames each (with batching, frames wait in the ring
-    # for a full launch and the finalize at the end of the timed region pairs the rest), so
-    # the algorithmic bytes of an average launch are the model's bytes per frame x the
-    # frames per launch.
-    lag_ms, lag_n = ktimes["lag"]
-    lag_avg_s = lag_ms / 1000.0 / max(lag_n, 1)
-    frames_per_launch = args.steps * CHUNK / max(lag_n, 1)
-    bytes_per_launch = lag_bytes_per_frame(T) * frames_per_launch
+    # Roofline of the lag kernel: its compulsory bytes (counted by the engine per launch) over
+    # its CUDA-event time on the engine's stream, against the measured copy bandwidth.
+    lag_ms, lag_n, lag_bytes = kstats["lag"]
+    fft_ms, fft_n, fft_bytes = kstats["fft"]
+    frames_timed = args.steps * CHUNK
+    lag_s = lag_ms / 1000.0
     hbm_peak, peak_kind = measured_peaks()
-    achieved = bytes_per_launch / lag_avg_s / 1e9
-    # The model's bytes assume one partner read per (frame, tau); the kernel reads each
-    # distinct partner frame of a launch once, so beside the model's fraction (above 1) the
-    # DRAM traffic ncu measured per launch over the same live launch time is reported.
-    traffic = profiled_traffic(frames_per_launch)
-    dram_gbs = traffic / lag_avg_s / 1e9 if traffic else None
+    achieved = lag_bytes / lag_s / 1e9
+    model_gbs = model_bytes_per_frame(w) * frames_timed / lag_s / 1e9
+    traffic_total, traffic_src = profiled_traffic(w, frames_timed)
+    per_launch = max(lag_n, 1)
 
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        line = {"metric": metric(w), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "multiscale_1024_4scales_64tau" if SIDE == 1024 else
-                           "small_512_4scales_64tau (profiling)", "frames": N_FRAMES, "side": SIDE,
-                           "scales": SCALES, "taus": T, "tau_max": max(taus), "lambdas": len(lambdas),
-                           "chunk": CHUNK, "lag_batch_frames": args.lag_batch or 32,
-                           "estimator": "unbiased", "steady_state": True,
-                           "l2": "inputs larger than L2 (ring of %d frames x %.1f MB)"
-                                 % (eng.info().ring_slots, frames_elements() * 8 / 1e6),
-                           "parallelism": f"replicas x{world} (independent streams, no collective)"},
-                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": CHUNK * SIDE * SIDE,
+                "config": config_of(w, world),
+                "impl_config": {"lag_batch_frames": eng.info().lag_batch_frames,
+                                "ring_slots": eng.info().ring_slots,
+                                "frame_spectra_mb": frames_elements(w) * 8 / 1e6},
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": CHUNK * side * side * bpp,
                         "d2h_bytes_per_step": isf_bufs[0].nbytes},
-                "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                             "frac": achieved / hbm_peak, "traffic": traffic,
-                             "traffic_gbs": dram_gbs, "traffic_frac": dram_gbs / hbm_peak if dram_gbs else None,
-                             "kernel": "lag_kernel", "peak_kind": peak_kind,
-                             "bytes_per_launch": bytes_per_launch, "frames_per_launch": frames_per_launch,
-                             "avg_launch_ms": lag_avg_s * 1000.0},
-                "kernels_ms": {k: {"total_ms": v[0], "launches": v[1]} for k, v in ktimes.items()},
+                "roofline": {"bound": "hbm", "kernel": "lag_pipe_kernel", "achieved": achieved, "peak": hbm_peak,
+                             "unit": "GB/s", "frac": achieved / hbm_peak, "peak_kind": peak_kind,
+                             "traffic": traffic_total / per_launch if traffic_total else None,
+                             "traffic_source": traffic_src,
+                             "bytes_per_launch": lag_bytes / per_launch, "launches": lag_n,
+                             "avg_launch_ms": lag_ms / per_launch,
+                             "frames_per_launch": frames_timed / per_launch,
+                             "model_bytes_per_frame": model_bytes_per_frame(w),
+                             "model_gbs": model_gbs, "model_frac": model_gbs / hbm_peak},
+                "fft_roofline": {"bound": "hbm", "achieved": fft_bytes / max(fft_ms, 1e-9) / 1e6,
+                                 "frac": fft_bytes / max(fft_ms, 1e-9) / 1e6 / hbm_peak, "unit": "GB/s",
+                                 "bytes": fft_bytes, "ms": fft_ms, "launches": fft_n},
+                "kernels_ms": {k: {"total_ms": v[0], "launches": v[1], "compulsory_bytes": v[2]}
+                               for k, v in kstats.items()},
                 "gpu_launches": int(launches), "clocks": clocks}
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline()
+            line["cpu_baseline"] = cpu_baseline(w, 1002)
         print(json.dumps(line), flush=True)
     eng.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def job_throughput(times_ms, frames_per_rank: int, world: int, device=None):
+    """Whole-job throughput of `world` ranks that each analysed frames_per_rank frames:
+    every timing is reduced to its maximum over ranks (the job ends when the slowest rank
+    does). Returns (value, e2e_value, max_ms, max_e2e_ms) for times_ms = [device, e2e]."""
+    import torch
+    t = torch.tensor(times_ms, dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total = frames_per_rank * world
+    return total / (float(t[0]) / 1000.0), total / (float(t[1]) / 1000.0), float(t[0]), float(t[1])
 
 
 def run_serving(args) -> None:
@@ -373,9 +490,10 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--lag-batch", type=int, default=0,
                     help="frames paired per lag-kernel launch (1..64; 0 = the engine default, 32)")
-    ap.add_argument("--workload", choices=["multiscale", "small", "serving"], default="multiscale",
-                    help="small: 512^2 frames, scales 512..64, same taus and chunk (profiling only); "
-                         "serving: many camera streams through one server (its own JSON line)")
+    ap.add_argument("--workload", choices=["c1", "c2", "c3", "c4", "multiscale", "small", "serving"], default="c2",
+                    help="c2 (default): the headline 1024^2 x 4-scale x 64-tau workload; c1, c3, c4: the other "
+                         "configurations; small: 512^2 frames with c2's taus (profiling only); serving: many "
+                         "camera streams through one server (its own JSON line)")
     ap.add_argument("--camera-fps", type=float, nargs="+", default=[30.0, 120.0, 480.0],
                     help="serving: camera frame rates to run (30 fps = one 30-frame chunk per second)")
     ap.add_argument("--periods", type=float, default=20.0, help="serving: chunk periods of arrivals")
@@ -383,14 +501,13 @@ def main() -> None:
     if args.workload == "serving":
         run_serving(args)
         return
-    if args.workload == "small":
-        globals().update(SMALL)
     if args.warmup < 3:
         args.warmup = 3
+    w = WORKLOADS[args.workload]
     if args.impl == "reference":
-        run_reference(args)
+        run_reference(args, w)
     else:
-        run_ours(args)
+        run_ours(args, w)
 
 
 if __name__ == "__main__":

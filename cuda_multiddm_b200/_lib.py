@@ -16,6 +16,7 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of device mem
           5: "frames missing", 6: "no suitable CUDA device", 7: "I/O error", 8: "busy"}
 
 PIX_BYTE0, PIX_U16LE = 0, 1
+FAULT_NONE, FAULT_LAG_WAIT = 0, 1
 EST_COMPAT, EST_UNBIASED = 0, 1
 
 
@@ -110,11 +111,14 @@ SIGNATURES = {
     "ddm_get_info": (C.c_int, [C.c_void_p, C.POINTER(Info)]),
     "ddm_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
     "ddm_kernel_times": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ddm_kernel_stats": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ddm_build_masks": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_float, C.c_void_p, C.c_void_p]),
     "ddm_compat_schedule": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ddm_lag_accumulate_static": (C.c_int, [C.c_void_p, C.c_int, C.c_longlong, C.c_void_p, C.c_void_p, C.c_int,
                                             C.c_void_p, C.c_int, C.c_void_p]),
+    "ddm_set_wait_limit": (C.c_int, [C.c_void_p, C.c_longlong]),
+    "ddm_inject_fault": (C.c_int, [C.c_void_p, C.c_int]),
     "ddm_host_alloc": (C.c_void_p, [C.c_size_t]),
     "ddm_host_free": (None, [C.c_void_p]),
     "ddm_last_error": (C.c_char_p, []),

@@ -138,6 +138,8 @@ struct ddm_engine {
     cudaEvent_t ev_isf_ready = nullptr, ev_isf_read = nullptr;
     double *fit_d = nullptr;                // ISF fitting: means, tau, q, curve fits, D (first fit call)
     int *status_d = nullptr;                // set by kernels whose bounded waits ran out
+    long long wait_cycles = kWaitCycles;    // limit of every lag-pipeline wait (ddm_set_wait_limit)
+    int inject = DDM_FAULT_NONE;            // one-shot fault for the next lag launch (ddm_inject_fault)
     LagMaps maps;                           // 2-D tensor maps of the ring for the lag kernel
     bool defer_lag = false;                 // served: lag launches are collected, not issued
     std::vector<DeferredLag> deferred;
@@ -168,6 +170,10 @@ struct ddm_engine {
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tev[3];
     long tlaunch[3] = {0, 0, 0};
+    // compulsory DRAM bytes of the kernels launched since the last ddm_kernel_stats: what
+    // each kernel must move at least (its inputs read once, its outputs written once)
+    double tbytes[3] = {0.0, 0.0, 0.0};
+    double az_bytes = 0.0;  // per azimuthal average: every masked accumulator element, all taus
 };
 
 namespace {
@@ -331,6 +337,9 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
         CUDA_TRY(cudaGetLastError());
         e->launches += 2;
         tr.e->tlaunch[0] += 2;
+        // the ROI's pixels read once and the frame's spectra written once
+        e->tbytes[0] += static_cast<double>(nf) *
+                        (static_cast<double>(e->M) * e->M * e->bpp + static_cast<double>(frame_bytes));
     }
     tr.end(0);
     return DDM_OK;
@@ -349,6 +358,18 @@ int launch_lag(ddm_engine *e, const Launch &L) {
     if (!err.empty()) return fail(DDM_ERR_STATE, "internal: " + err);
     const int ntab = static_cast<int>(table.size());
     if (ntab > e->tab_stride) return fail(DDM_ERR_STATE, "internal: lag table overflow");
+    if (e->inject == DDM_FAULT_LAG_WAIT) {
+        // Test of the error path: the last entry's window is moved to start at the end of
+        // the partner list, so it reaches groups the producer never issues and the
+        // consumers' waits run out. Every entry becomes a single full window (no fused
+        // runs, no per-slot checks), so every shared-memory offset stays masked to the ring
+        // and the kernel reads nothing outside its table.
+        int *ent_ub = table.data() + kTabEntries + L.ent_acc.size();
+        int *ent_full = ent_ub + L.ent_acc.size();
+        for (size_t i = 0; i < L.ent_acc.size(); i++) ent_full[i] = kLagFullFlag;
+        ent_ub[L.ent_acc.size() - 1] = table[kTabNgroups] * kLagGroup;
+        e->inject = DDM_FAULT_NONE;
+    }
     const int ts = e->tab_next;
     e->tab_next = (e->tab_next + 1) % kTables;
     if (e->tab_used[ts]) CUDA_TRY(cudaEventSynchronize(e->tab_ev[ts]));
@@ -379,7 +400,8 @@ int launch_lag(ddm_engine *e, const Launch &L) {
 #define LAG_CASE(JJ)                                                                                   \
     case JJ:                                                                                           \
         lag_pipe_kernel<JJ><<<grid, kLagThreads, smem, e->stream>>>(e->ring, e->acc, e->E, td, e->status_d, \
-                                                                     e->maps, static_cast<int>(blocks)); \
+                                                                     e->maps, static_cast<int>(blocks),  \
+                                                                     e->wait_cycles);                    \
         break;
         LAG_CASE(4) LAG_CASE(8) LAG_CASE(16) LAG_CASE(20) LAG_CASE(24) LAG_CASE(30) LAG_CASE(32) LAG_CASE(64)
 #undef LAG_CASE
@@ -389,6 +411,15 @@ int launch_lag(ddm_engine *e, const Launch &L) {
     CUDA_TRY(cudaEventRecord(e->tab_free[ts], e->stream));
     tr.end(1);
     e->launches++;
+    {
+        // every register frame and every distinct partner frame of the launch read once, every
+        // accumulator row read and written once
+        int frames = 0;
+        for (int j = 0; j < L.nreg; j++) frames += L.reg[j] >= 0;
+        const int *uslot = table.data() + kTabEntries + 3 * table[kTabNtau];
+        for (int u = 0; u < table[kTabNunion]; u++) frames += uslot[u] >= 0;
+        e->tbytes[1] += 8.0 * static_cast<double>(e->E) * (frames + 2.0 * table[kTabNtau]);
+    }
     return DDM_OK;
 }
 
@@ -507,6 +538,7 @@ int run_azimuth(ddm_engine *e, const std::vector<double> &norm) {
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaEventRecord(e->norm_free[ns], e->stream));
     tr.end(a.items > 0 ? 2 : 1);
+    e->tbytes[2] += e->az_bytes;
     e->launches += a.items > 0 ? 2 : 1;
     return DDM_OK;
 }
@@ -783,6 +815,7 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
             items += static_cast<long long>(d.tiles) * e->T * nloc;
             idx_all.insert(idx_all.end(), idx.begin(), idx.end());
             e->counts_h.insert(e->counts_h.end(), counts.begin(), counts.end());
+            e->az_bytes += 8.0 * e->T * static_cast<double>(idx.size()) * d.tiles;
             e->q_ptr_s.push_back(qp);
             e->idx_s.push_back(std::move(idx));
         }
@@ -1227,6 +1260,25 @@ extern "C" int ddm_get_info(const ddm_engine *e, ddm_info *info) {
 
 extern "C" const char *ddm_last_error(void) { return last_error(); }
 
+extern "C" int ddm_set_wait_limit(ddm_engine *e, long long cycles) {
+    clear_error();
+    if (!e) return fail(DDM_ERR_INVALID_ARG, "null engine");
+    if (cycles < 0) return fail(DDM_ERR_INVALID_ARG, "ddm_set_wait_limit: cycles must be >= 0");
+    e->wait_cycles = cycles == 0 ? kWaitCycles : cycles;
+    return DDM_OK;
+}
+
+extern "C" int ddm_inject_fault(ddm_engine *e, int fault) {
+    clear_error();
+    if (!e) return fail(DDM_ERR_INVALID_ARG, "null engine");
+    if (fault != DDM_FAULT_NONE && fault != DDM_FAULT_LAG_WAIT)
+        return fail(DDM_ERR_INVALID_ARG, "ddm_inject_fault: unknown fault");
+    if (fault == DDM_FAULT_LAG_WAIT && e->defer_lag)
+        return fail(DDM_ERR_STATE, "ddm_inject_fault: not for served streams");
+    e->inject = fault;
+    return DDM_OK;
+}
+
 extern "C" int ddm_set_timing(ddm_engine *e, int enabled) {
     if (!e) return fail(DDM_ERR_INVALID_ARG, "null engine");
     e->timing = enabled != 0;
@@ -1234,8 +1286,16 @@ extern "C" int ddm_set_timing(ddm_engine *e, int enabled) {
 }
 
 extern "C" int ddm_kernel_times(ddm_engine *e, double *ms, long *launches) {
+    return ddm_kernel_stats(e, ms, launches, nullptr);
+}
+
+extern "C" int ddm_kernel_stats(ddm_engine *e, double *ms, long *launches, double *bytes) {
     clear_error();
     if (!e || !ms || !launches) return fail(DDM_ERR_INVALID_ARG, "bad argument");
+    for (int g = 0; g < 3; g++) {
+        if (bytes) bytes[g] = e->tbytes[g];
+        e->tbytes[g] = 0.0;
+    }
     CUDA_TRY(cudaStreamSynchronize(e->stream));
     for (int g = 0; g < 3; g++) {
         double total = 0.0;

@@ -36,9 +36,11 @@
 // the consumers release every group of a block at its end), and as the CTAs retire the SMs
 // pass to the next piece's FFT on the other stream instead of to further lag blocks.
 //
-// Every mbarrier wait is bounded (kWaitCycles clock cycles); a wait that runs out
-// sets *status to 1, and the CTA waits (bounded again) for its own copies in flight before
-// returning, so a broken schedule ends the kernel instead of hanging the GPU.
+// Every mbarrier wait of the pipeline is bounded (wait_cycles clock cycles, a launch
+// argument, kWaitCycles by default); a wait that runs out sets *status to 1, and the CTA
+// waits for its own copies in flight (bounded by kWaitCycles, whatever the launch's limit,
+// so no CTA exits while a copy into its shared memory may still land) before returning: a
+// broken schedule ends the kernel instead of hanging the GPU.
 #pragma once
 
 #include <cstdint>
@@ -144,11 +146,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
 // Bounded wait: false if the phase did not complete within kWaitCycles SM clocks (about
 // 0.2 s at 2 GHz, four orders of magnitude above any legitimate copy latency).
 constexpr long long kWaitCycles = 400000000LL;
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, long long limit = kWaitCycles) {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity))
-        if (clock64() - t0 > kWaitCycles) return false;
+        if (clock64() - t0 > limit) return false;
     return true;
 }
 
@@ -191,7 +193,8 @@ struct LagMaps {
 template <int J>
 __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, float2 *__restrict__ acc, long long E,
                                               const int *__restrict__ table, int *__restrict__ status,
-                                              const LagMaps &maps, int block_begin, int block_end, int block_step) {
+                                              const LagMaps &maps, int block_begin, int block_end, int block_step,
+                                              long long wait_cycles) {
     constexpr int kLanes = lag_lanes(J);
     constexpr int kJT = J / kLanes;  // register frames per thread
     constexpr int kElems = lag_cta_elems(J);
@@ -240,7 +243,7 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
             long long e0 = static_cast<long long>(block_begin) * kElems;
             for (int G = 0, g = 0, block = block_begin; block < block_end; G++) {
                 const int gs = G & (kGS - 1), fill = G / kGS;
-                if (fill > 0 && !mbar_wait_bounded(&empty[gs], (fill - 1) & 1)) {
+                if (fill > 0 && !mbar_wait_bounded(&empty[gs], (fill - 1) & 1, wait_cycles)) {
                     *abort_flag = 1;
                     break;
                 }
@@ -304,7 +307,7 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
                 bool ok = true;
                 for (; waited <= glast; waited++) {
                     const int G = Gbase + waited;
-                    if (!mbar_wait_bounded(&full[G & (kGS - 1)], (G / kGS) & 1)) {
+                    if (!mbar_wait_bounded(&full[G & (kGS - 1)], (G / kGS) & 1, wait_cycles)) {
                         ok = false;
                         break;
                     }
@@ -410,7 +413,7 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
             // groups no window reached (none in tables of the host's builder): wait and release
             for (; waited < ngroups; waited++) {
                 const int G = Gbase + waited;
-                if (!mbar_wait_bounded(&full[G & (kGS - 1)], (G / kGS) & 1)) {
+                if (!mbar_wait_bounded(&full[G & (kGS - 1)], (G / kGS) & 1, wait_cycles)) {
                     *abort_flag = 1;
                     break;
                 }
@@ -441,8 +444,9 @@ template <int J>
 __global__ void __launch_bounds__(kLagThreads, kLagCtasPerSm)
     lag_pipe_kernel(const float2 *__restrict__ ring, float2 *__restrict__ acc, long long E,
                     const int *__restrict__ table, int *__restrict__ status, const __grid_constant__ LagMaps maps,
-                    int nblocks) {
-    lag_pipe_body<J>(ring, acc, E, table, status, maps, static_cast<int>(blockIdx.x), nblocks, static_cast<int>(gridDim.x));
+                    int nblocks, long long wait_cycles) {
+    lag_pipe_body<J>(ring, acc, E, table, status, maps, static_cast<int>(blockIdx.x), nblocks, static_cast<int>(gridDim.x),
+                     wait_cycles);
 }
 
 // The lag work of several engines (served streams) in one launch: item i owns CTAs
@@ -470,7 +474,7 @@ __global__ void __launch_bounds__(kLagThreads, kLagCtasPerSm)
     }
     const LagBatchItem &it = items[lo];
     const int b = static_cast<int>(blockIdx.x) - it.cta_begin;
-    lag_pipe_body<J>(it.ring, it.acc, it.E, it.table, it.status, *it.maps, b, b + 1, 1);
+    lag_pipe_body<J>(it.ring, it.acc, it.E, it.table, it.status, *it.maps, b, b + 1, 1, kWaitCycles);
 }
 
 // Dynamic shared memory of a launch of lag_pipe_kernel<J> with a table of table_ints ints

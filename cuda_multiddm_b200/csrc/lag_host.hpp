@@ -116,15 +116,18 @@ inline int lag_pick_j(int nreg) {
 // Tensor maps of a ring float2[slots][E] for boxes of 128 or 64 elements (the element blocks
 // of the one- and two-lane kernels) x 1, 2, 4, 8 slots.
 inline std::string make_lag_maps(const void *ring, long long E, int slots, LagMaps *maps) {
-    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-    if (!encode) {
+    // looked up once, by a thread-safe static initialiser (engines on several threads and
+    // the static entry point all come through here)
+    static const PFN_cuTensorMapEncodeTiled_v12000 encode = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
         cudaDriverEntryPointQueryResult q;
         void *fn = nullptr;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
             q != cudaDriverEntryPointSuccess || !fn)
-            return "cuTensorMapEncodeTiled is not available from the driver";
-        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-    }
+            return nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }();
+    if (!encode) return "cuTensorMapEncodeTiled is not available from the driver";
+    if (reinterpret_cast<uintptr_t>(ring) % 16 != 0) return "the ring must start on a 16-byte boundary";
     if ((E * 8) % 16 != 0) return "frame size must be a multiple of 16 bytes for the ring tensor maps";
     const cuuint64_t dims[2] = {static_cast<cuuint64_t>(E), static_cast<cuuint64_t>(slots)};
     const cuuint64_t strides[1] = {static_cast<cuuint64_t>(E) * 8};

@@ -157,6 +157,14 @@ class Engine:
     def synchronize(self) -> None:
         check(lib().ddm_synchronize(self._h))
 
+    def set_wait_limit(self, cycles: int) -> None:
+        """Limit of every lag-pipeline wait in SM clock cycles (0 = the default, ~0.2 s)."""
+        check(lib().ddm_set_wait_limit(self._h, int(cycles)))
+
+    def inject_fault(self, fault: int) -> None:
+        """Test hook: make the next lag launch's waits run out (FAULT_LAG_WAIT)."""
+        check(lib().ddm_inject_fault(self._h, int(fault)))
+
     def reset(self) -> None:
         check(lib().ddm_reset_accumulators(self._h))
 
@@ -237,10 +245,15 @@ class Engine:
 
     def kernel_times(self) -> dict:
         """{group: (device ms, launches)} since the last call; groups fft, lag, azimuth."""
+        return {g: v[:2] for g, v in self.kernel_stats().items()}
+
+    def kernel_stats(self) -> dict:
+        """{group: (device ms, launches, compulsory DRAM bytes)} since the last call."""
         ms = np.zeros(3, np.float64)
         n = np.zeros(3, np.int64)
-        check(lib().ddm_kernel_times(self._h, ms.ctypes.data, n.ctypes.data))
-        return {g: (float(ms[i]), int(n[i])) for i, g in enumerate(("fft", "lag", "azimuth"))}
+        b = np.zeros(3, np.float64)
+        check(lib().ddm_kernel_stats(self._h, ms.ctypes.data, n.ctypes.data, b.ctypes.data))
+        return {g: (float(ms[i]), int(n[i]), float(b[i])) for i, g in enumerate(("fft", "lag", "azimuth"))}
 
     def info(self) -> Info:
         inf = Info()

@@ -239,6 +239,12 @@ int ddm_get_info(const ddm_engine *e, ddm_info *info);
  * milliseconds and the number of launches since the last call, and clears them. */
 int ddm_set_timing(ddm_engine *e, int enabled);
 int ddm_kernel_times(ddm_engine *e, double *ms_out, long *launches_out);
+/* As ddm_kernel_times, also returning per group the compulsory DRAM bytes of the kernels
+ * launched since the last call (counted whether timing is on or not): FFT, the ROI's pixels
+ * read once and every spectrum written once; lag, each register frame and each distinct
+ * partner frame of a launch read once and each accumulator row read and written once;
+ * azimuth, every masked accumulator element of every tau read once. bytes_out may be NULL. */
+int ddm_kernel_stats(ddm_engine *e, double *ms_out, long *launches_out, double *bytes_out);
 
 /* Host-only helpers (no GPU needed). ddm_build_masks: the annulus masks of one scale,
  * [lambda][ky][kx] bytes (kx in [0, s/2]; mask_out may be NULL) and per-lambda pixel
@@ -279,6 +285,24 @@ int ddm_lag_accumulate_static(const void *ring, int ring_slots, long long elemen
 /* Page-locked host memory for frame buffers (asynchronous copies); NULL on failure. */
 void *ddm_host_alloc(size_t bytes);
 void ddm_host_free(void *ptr);
+
+/* Bounded waits. Every wait in the lag kernel's copy pipeline gives up after `cycles` SM
+ * clock cycles (0 = the default, 400,000,000: about 0.2 s at 1.965 GHz, orders of magnitude
+ * above any legitimate copy latency). A wait that runs out makes the kernel finish its copies
+ * in flight and return with a device status that the next ddm_finalize, ddm_synchronize or
+ * ddm_wait_isf reports as DDM_ERR_CUDA ("... wait timed out ..."); the CUDA context stays
+ * usable. The reference has no such path: every error there ends the process
+ * (src/debug.cpp:10-15). */
+int ddm_set_wait_limit(ddm_engine *e, long long cycles);
+
+/* Fault injection for tests of the error path (no counterpart in the reference).
+ * DDM_FAULT_LAG_WAIT: the engine's next lag launch gets a pair table whose last tau window
+ * reaches a group of partner frames that is never copied, so that launch's pipeline waits
+ * run out and the error surfaces as above. Nothing faults on the GPU: every access of the
+ * altered launch stays inside its buffers and every wait is bounded. One-shot; not for
+ * streams of a server. */
+typedef enum { DDM_FAULT_NONE = 0, DDM_FAULT_LAG_WAIT = 1 } ddm_fault;
+int ddm_inject_fault(ddm_engine *e, int fault);
 
 /* Text of the last error on this thread. */
 const char *ddm_last_error(void);

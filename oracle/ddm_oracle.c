@@ -363,12 +363,25 @@ static int ddm_run_impl(const unsigned char *frames, int nframes, int w, int h, 
             }
             for (int t = 0; t < T; t++) norm[t] = (double)N; /* DDM.cu:875, :92 */
         } else {
-            for (int t = 0; t < T; t++) {
-                for (int a = 0; a + taus[t] < N; a++)
-                    accumulate_pair(acc + (long)t * fsz, spec + 2 * (size_t)a * fsz,
-                                    spec + 2 * (size_t)(a + taus[t]) * fsz, fsz, inv_s4);
-                norm[t] = N - taus[t] > 0 ? (double)(N - taus[t]) : 0.0;
+            /* Every pair (a, a + tau) with a + tau < N. Blocked over elements so that a block's
+             * frames stay in cache across all taus; each element still adds its pairs tau by tau,
+             * a ascending, so the sums are those of the plain loop bit for bit. */
+            const long KB = 256;
+#pragma omp parallel for schedule(dynamic)
+            for (long k0 = 0; k0 < fsz; k0 += KB) {
+                const long k1 = k0 + KB < fsz ? k0 + KB : fsz;
+                for (int t = 0; t < T; t++) {
+                    double *at = acc + (long)t * fsz;
+                    for (int a = 0; a + taus[t] < N; a++) {
+                        const double *fa = spec + 2 * (size_t)a * fsz, *fb = spec + 2 * (size_t)(a + taus[t]) * fsz;
+                        for (long k = k0; k < k1; k++) {
+                            double dr = fa[2 * k] - fb[2 * k], di = fa[2 * k + 1] - fb[2 * k + 1];
+                            at[k] += (dr * dr + di * di) * inv_s4;
+                        }
+                    }
+                }
             }
+            for (int t = 0; t < T; t++) norm[t] = N - taus[t] > 0 ? (double)(N - taus[t]) : 0.0;
         }
         orc_azimuthal(acc, s, tiles, T, lambdas, Q, tolerance, norm, isf + isf_off);
         isf_off += (long)tiles * Q * T;
@@ -416,7 +429,7 @@ static double now_s(void) {
 
 double orc_bench_steady(const unsigned char *frames, int nframes, int w, int h, int bpp,
                         int pixmode, const int *scales, int S, const int *taus, int T,
-                        int timed_frames, int threads) {
+                        int warm_frames, int timed_frames, int threads) {
 #ifdef _OPENMP
     if (threads > 0) omp_set_num_threads(threads);
 #else
@@ -453,8 +466,9 @@ double orc_bench_steady(const unsigned char *frames, int nframes, int w, int h, 
         for (int f = warm; f < R; f++)
             memcpy(ring + 2 * (size_t)f * fsz, ring + 2 * (size_t)(f % warm) * fsz,
                    sizeof(double) * 2 * fsz);
-        double t0 = now_s();
-        for (int i = 0; i < timed_frames; i++) {
+        double t0 = 0.0;
+        for (int i = 0; i < warm_frames + timed_frames; i++) {
+            if (i == warm_frames) t0 = now_s();
             const int b = R + i; /* frame number; ring slot b % R */
             double *fb = ring + 2 * (size_t)(b % R) * fsz;
             orc_extract(frames + frame_bytes * (i % nframes), w, h, bpp, pixmode, 0, 0, M, s, px);
@@ -471,4 +485,14 @@ double orc_bench_steady(const unsigned char *frames, int nframes, int w, int h, 
         free(px);
     }
     return total;
+}
+
+/* FNV-1a (64-bit) over n bytes: the hash the reference harness prints for each mask. */
+uint64_t orc_fnv1a(const unsigned char *bytes, long n) {
+    uint64_t h = 1469598103934665603ULL;
+    for (long i = 0; i < n; i++) {
+        h ^= bytes[i];
+        h *= 1099511628211ULL;
+    }
+    return h;
 }

@@ -26,6 +26,8 @@
 #ifndef DDM_ORACLE_H
 #define DDM_ORACLE_H
 
+#include <stdint.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -103,13 +105,25 @@ void orc_azimuthal(const double *acc, int scale, int tiles, int tau_count, const
                    int lambda_count, float tolerance, const double *norm, double *out);
 
 /* Steady-state throughput sample of the causal (unbiased) path on the CPU: every
- * timed frame is extracted, transformed at every scale and paired with the frames
- * at each tau before it, FP64, OpenMP over elements with `threads` threads (0 = all).
- * The ring is first filled with copies of transformed frames (untimed). Returns the
- * wall time in seconds of the timed frames. */
+ * frame is extracted, transformed at every scale and paired with the frames at each tau
+ * before it, FP64, OpenMP over tiles/elements with `threads` threads (0 = all). The ring
+ * is first filled with copies of transformed frames, then `warm_frames` frames run
+ * untimed, then `timed_frames` frames (frame i of the sample is frames[i % nframes]).
+ * Returns the wall time in seconds of the timed frames (summed over the scales, which
+ * run one after another). */
 double orc_bench_steady(const unsigned char *frames, int nframes, int w, int h, int bpp,
                         int pixmode, const int *scales, int scale_count, const int *taus,
-                        int tau_count, int timed_frames, int threads);
+                        int tau_count, int warm_frames, int timed_frames, int threads);
+
+/* 64-bit FNV-1a over n bytes (the hash the reference harness prints for each mask). */
+uint64_t orc_fnv1a(const unsigned char *bytes, long n);
+
+/* The synthetic particle video of the benchmark and the tests, restated from the product's
+ * generator (ddm_synth_video, same arguments, bit-identical bytes) so that the CPU arms do
+ * not load the product library. Returns 0, or a negative error. */
+int orc_synth_video(uint64_t seed, int width, int height, int frames, int spots, double spot_sigma,
+                    double amplitude, double background, double step_var, double step_var_b,
+                    double noise_sd, int max_value, unsigned char *out);
 
 #ifdef __cplusplus
 }

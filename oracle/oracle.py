@@ -25,9 +25,7 @@ _lib = None
 
 def build() -> None:
     """Compile liboracle.so (and the reference program when its sources exist here)."""
-    subprocess.run(["make", "-s", "-C", str(HERE), "oracle"], check=True)
-    if Path("/root/reference/src/DDM.cu").exists():
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
+    subprocess.run(["make", "-s", "-C", str(HERE), "oracle", "ref-if-present"], check=True)
 
 
 def lib() -> C.CDLL:
@@ -62,7 +60,12 @@ def lib() -> C.CDLL:
         l.orc_azimuthal.argtypes = [P, C.c_int, C.c_int, C.c_int, P, C.c_int, C.c_float, P, P]
         l.orc_bench_steady.restype = C.c_double
         l.orc_bench_steady.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_int, P, C.c_int,
-                                       C.c_int, C.c_int]
+                                       C.c_int, C.c_int, C.c_int]
+        l.orc_fnv1a.restype = C.c_uint64
+        l.orc_fnv1a.argtypes = [P, C.c_long]
+        l.orc_synth_video.restype = C.c_int
+        l.orc_synth_video.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                      C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, P]
         _lib = l
     return _lib
 
@@ -196,10 +199,39 @@ def azimuthal(acc: np.ndarray, scale: int, tiles: int, lambdas, tol: float, norm
     return out
 
 
-def bench_steady(frames: np.ndarray, scales, taus, timed_frames: int, threads: int = 0) -> float:
-    fr = np.ascontiguousarray(frames, dtype=np.uint8)
+def bench_steady(frames: np.ndarray, scales, taus, timed_frames: int, threads: int = 0, warm_frames: int = 0,
+                 pixmode: int = PIX_BYTE0) -> float:
+    """Seconds the FP64 path takes for `timed_frames` steady-state frames (after
+    `warm_frames` untimed ones); uint8 or uint16 (little-endian) frames [n, h, w]."""
+    fr = np.ascontiguousarray(frames)
     n, h, w = fr.shape
+    bpp = 2 if fr.dtype == np.uint16 else 1
+    raw = fr.view(np.uint8)
     s = _i32(scales)
     t = _i32(taus)
-    return float(lib().orc_bench_steady(fr.ctypes.data, n, w, h, 1, PIX_BYTE0, s.ctypes.data, len(s), t.ctypes.data,
-                                        len(t), timed_frames, threads))
+    r = float(lib().orc_bench_steady(raw.ctypes.data, n, w, h, bpp, pixmode, s.ctypes.data, len(s), t.ctypes.data,
+                                     len(t), warm_frames, timed_frames, threads))
+    if r < 0:
+        raise MemoryError("orc_bench_steady: host allocation failed")
+    return r
+
+
+def fnv1a(data: np.ndarray) -> int:
+    """64-bit FNV-1a over the bytes of `data` (C order)."""
+    b = np.ascontiguousarray(data).view(np.uint8)
+    return int(lib().orc_fnv1a(b.ctypes.data, b.size))
+
+
+def synth_video(seed: int, width: int, height: int, frames: int, spots: int, *, spot_sigma: float = 2.0,
+                amplitude: float = 120.0, background: float = 20.0, step_var: float = 0.5,
+                step_var_b: float | None = None, noise_sd: float = 4.0, max_value: int = 255) -> np.ndarray:
+    """The product generator's video (same arguments and defaults as
+    cuda_multiddm_b200.media.synth_video), made by the oracle's own restatement."""
+    dt = np.uint8 if max_value <= 255 else np.uint16
+    out = np.zeros((frames, height, width), dt)
+    st = lib().orc_synth_video(seed, width, height, frames, spots, spot_sigma, amplitude, background, step_var,
+                               step_var if step_var_b is None else step_var_b, noise_sd, max_value,
+                               out.ctypes.data)
+    if st != 0:
+        raise RuntimeError(f"orc_synth_video failed with {st}")
+    return out

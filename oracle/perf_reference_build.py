@@ -4,7 +4,7 @@ GPU, with the same flags, in the reference's own benchmark mode (-B: synthetic f
 file input), and prints one JSON line per configuration. Run on a GPU host from the
 repository root:
 
-    python tests/perf_reference_build.py
+    python oracle/perf_reference_build.py
 
 Only configurations whose scales are single-tile are run: the reference's final analysis
 reads its accumulator at n*(tile*T + tau*tiles) (src/DDM.cu:122 with

@@ -342,3 +342,28 @@ def test_kernel_launches_counted():
     # (launches take up to 32 frames); then the two azimuthal stages
     assert info.kernel_launches == 2 * 2 + 1 + 2
     assert lib() is not None
+
+
+def test_wait_timeout_is_reported_and_device_stays_usable():
+    """The lag kernel's bounded waits: a pair table whose last window reaches a group of
+    partner frames that is never copied (host-side fault injection) makes the pipeline waits
+    run out after a short limit; the kernel returns a status instead of hanging, finalize
+    reports DDM_ERR_CUDA, and the next engine on the device computes correct results."""
+    from cuda_multiddm_b200._lib import FAULT_LAG_WAIT
+    frames = media.synth_video(5, 64, 64, 20, 20, step_var=1.0)
+    scales, taus, lambdas = [64, 32], [1, 2, 3, 5], [4.0, 8.0, 16.0]
+    cfg = EngineConfig(frame_width=64, frame_height=64, scales=scales, taus=taus, lambdas=lambdas,
+                       chunk_frames=10, estimator="unbiased")
+    with Engine(cfg) as eng:
+        eng.set_wait_limit(2_000_000)  # about 1 ms of SM clocks
+        eng.inject_fault(FAULT_LAG_WAIT)
+        eng.submit(frames)
+        with pytest.raises(DDMError) as info:
+            eng.finalize()
+        assert info.value.status == 2 and "timed out" in str(info.value)
+    with Engine(cfg) as eng:
+        eng.submit(frames)
+        eng.finalize()
+        got = eng.isf()
+    want, _ = O.ddm_run(frames, scales, taus, lambdas, estimator=O.EST_UNBIASED, chunk=10)
+    assert_isf_close(got, want, scales, len(lambdas), len(taus))

@@ -152,3 +152,37 @@ def test_log_lists():
     assert len(set(media.log_taus(1, 300, 48))) == 48 and media.log_taus(1, 400, 64)[-1] == 400
     lam = media.log_lambdas(2, 512, 30)
     assert len(lam) == 30 and abs(lam[0] - 2) < 1e-6 and abs(lam[-1] - 512) < 1e-3
+
+
+@pytest.mark.parametrize("idx", [4, 5])
+def test_engine_masks_match_reference_hashes(idx):
+    """The engine's own mask builder at s = 1024 and 2048 against the counts and FNV-1a hashes
+    the reference's buildAzimuthMask produced (tests/golden/reference_outputs.json)."""
+    import json
+    from cases import MASK_CASES
+    g = json.loads((ROOT / "tests" / "golden" / "reference_outputs.json").read_text())["masks"][idx]
+    scale, tol, _ = MASK_CASES[idx]
+    assert g["scale"] == scale
+    lam = np.asarray(g["lambdas"], np.float32)
+    m = np.zeros((len(lam), scale, scale // 2 + 1), np.uint8)
+    c = np.zeros(len(lam), np.int32)
+    assert lib().ddm_build_masks(scale, lam.ctypes.data, len(lam), C.c_float(tol), m.ctypes.data,
+                                 c.ctypes.data) == 0
+    assert c.tolist() == g["counts"]
+    assert [str(O.fnv1a(m[q])) for q in range(len(lam))] == g["fnv"]
+
+
+@pytest.mark.parametrize("kw", [
+    dict(seed=3, width=96, height=64, frames=5, spots=40, step_var=2.0),
+    dict(seed=9, width=64, height=64, frames=4, spots=30, amplitude=2000.0, background=300.0, noise_sd=-1.0,
+         max_value=4095, step_var=0.4, step_var_b=4.0),
+    dict(seed=1002, width=128, height=128, frames=3, spots=60, step_var=2.0),
+])
+def test_oracle_generator_bit_identical_to_product(kw):
+    """The CPU arms make their input with the oracle's restatement of the generator (so they
+    never load the product library); it must give the product generator's bytes exactly."""
+    kw = dict(kw)
+    args = (kw.pop("seed"), kw.pop("width"), kw.pop("height"), kw.pop("frames"), kw.pop("spots"))
+    a = media.synth_video(*args, **kw)
+    b = O.synth_video(*args, **kw)
+    assert a.dtype == b.dtype and np.array_equal(a, b)
