@@ -352,8 +352,11 @@ int main(int argc, char **argv) {
         ddm_tuning tuned;
         if (ddm_autotune(&cfg, tune_cache.c_str(), &tuned) != DDM_OK) die(ddm_last_error());
         cfg.lag_batch_frames = tuned.lag_batch_frames;
+        cfg.lag_geometry = tuned.lag_geometry;
+        cfg.fft_group_frames = tuned.fft_group_frames;
         if (g_verbose)
-            std::fprintf(stderr, "[Info] lag_batch_frames %d (%s)\n", tuned.lag_batch_frames,
+            std::fprintf(stderr, "[Info] lag_batch_frames %d, lag_geometry %d, fft_group_frames %d (%s)\n",
+                         tuned.lag_batch_frames, tuned.lag_geometry, tuned.fft_group_frames,
                          tuned.from_cache ? "cached" : "timed");
     }
     ddm_engine *eng = nullptr;

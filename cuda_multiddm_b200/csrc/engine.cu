@@ -24,6 +24,7 @@
 #include "../../include/ddm.h"
 #include "errors.hpp"
 #include "host.hpp"
+#include "dft_bf16.cuh"
 #include "fft.cuh"
 #include "fit.cuh"
 #include "kernels.cuh"
@@ -103,6 +104,12 @@ struct ddm_engine {
     long long pieces = 0;
     int R = 0, jmax = 32;
     float2 *ring = nullptr, *acc = nullptr, *tw = nullptr;
+    // split-BF16 tensor-core DFT of the tiles of side 32, 64, 128 (ddm_config.small_tile_dft):
+    // its cos/sin tables per log2 s - 5, in the kernel's shared-memory layout
+    bool small_dft = false;
+    int lag_geom = 0;  // lag-kernel geometry for launches of up to 32 frames (ddm_config.lag_geometry)
+    int fft_group = 0;  // frames per FFT launch (ddm_config.fft_group_frames; 0 = the 256 MB rule)
+    uint4 *dft_tab[kDftMaxLog2 - kDftMinLog2 + 1] = {nullptr, nullptr, nullptr};
     uint8_t *stage = nullptr;
     int *tables_d = nullptr, *tables_h = nullptr;
     cudaEvent_t tab_ev[kTables] = {};    // table slot i uploaded (its pinned host copy is free again)
@@ -207,7 +214,7 @@ void free_all(ddm_engine *e) {
     if (e->stream && e->ev_isf_read) cudaStreamWaitEvent(e->stream, e->ev_isf_read, 0);  // a result copy reads isf_d
     void *dev[] = {e->ring, e->acc, e->tw, e->stage, e->tables_d, e->chunk_beg_d, e->chunk_end_d,
                    e->chunk_first_d, e->chunk_count_d, e->partial_d, e->idx_d, e->counts_d, e->norm_d,
-                   e->isf_d, e->fit_d, e->status_d};
+                   e->isf_d, e->fit_d, e->status_d, e->dft_tab[0], e->dft_tab[1], e->dft_tab[2]};
     cudaStream_t fs = e->stream ? e->stream : e->fft_stream;
     for (void *p : dev)
         if (p) cudaFreeAsync(p, fs);
@@ -294,8 +301,9 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
     rows.R = e->R;
     rows.tw = e->tw;
     cols = rows;
-    int row_ctas = 0, col_ctas = 0;
+    int row_ctas = 0, col_ctas = 0, nfft = 0;
     size_t smem = 0;
+    std::vector<FftScale> dft_scales;  // scales for the tensor-core DFT
     for (int si = 0; si < e->S; si++) {
         const ScaleDesc &d = e->sd[si];
         const int s = d.s, per = fft_per_cta(s), side = e->M / s;
@@ -306,23 +314,31 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
         fs.log2side = log2i(side);
         fs.n = d.n;
         fs.off = d.off;
+        if (e->small_dft && fs.log2s >= kDftMinLog2 && fs.log2s <= kDftMaxLog2) {
+            dft_scales.push_back(fs);
+            continue;
+        }
         fs.cta_begin = row_ctas;
         fs.ctas_per_frame = static_cast<int>((static_cast<long long>(d.tiles) * (s / 2) + per - 1) / per);
-        rows.sc[si] = fs;
+        rows.sc[nfft] = fs;
         row_ctas += fs.ctas_per_frame;
         fs.cta_begin = col_ctas;
         fs.ctas_per_frame = static_cast<int>((static_cast<long long>(d.tiles) * (s / 2 + 1) + per - 1) / per);
-        cols.sc[si] = fs;
+        cols.sc[nfft] = fs;
         col_ctas += fs.ctas_per_frame;
+        nfft++;
         smem = std::max(smem, fft_smem_bytes(s));
     }
+    rows.S = cols.S = nfft;
     // Frames go through both passes in groups of up to 256 MB of spectra (15 frames of the
     // 1024^2 x 4-scale shape): fewer, larger launches were measured faster than groups small
     // enough for the row pass's output to stay in L2 (frames/s at 34 / 64 / 100 / 256 MB:
     // 0.98 / 1 / 1.015 / 1.025), and two or more groups per piece keep the host copies of a
     // group overlapping the FFT of the one before (one group per piece: -6 % end to end).
     const long long frame_bytes = e->E * static_cast<long long>(sizeof(float2));
-    const int group = static_cast<int>(std::max<long long>(1, std::min<long long>(nframes, (256LL << 20) / frame_bytes)));
+    const int group = e->fft_group > 0 ? std::min(e->fft_group, nframes)
+                                       : static_cast<int>(std::max<long long>(
+                                             1, std::min<long long>(nframes, (256LL << 20) / frame_bytes)));
     for (int f0 = 0; f0 < nframes; f0 += group) {
         const int nf = std::min(group, nframes - f0);
         if (before_group) {
@@ -331,12 +347,43 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
         }
         rows.src = src + f0 * frame_stride;
         rows.first_label = cols.first_label = first_label + f0;
-        fft_rows_kernel<<<dim3(row_ctas, nf), kFftThreads, smem, e->fft_stream>>>(rows);
-        CUDA_TRY(cudaGetLastError());
-        fft_cols_kernel<<<dim3(col_ctas, nf), kFftThreads, smem, e->fft_stream>>>(cols);
-        CUDA_TRY(cudaGetLastError());
-        e->launches += 2;
-        tr.e->tlaunch[0] += 2;
+        if (nfft > 0) {
+            fft_rows_kernel<<<dim3(row_ctas, nf), kFftThreads, smem, e->fft_stream>>>(rows);
+            CUDA_TRY(cudaGetLastError());
+            fft_cols_kernel<<<dim3(col_ctas, nf), kFftThreads, smem, e->fft_stream>>>(cols);
+            CUDA_TRY(cudaGetLastError());
+            e->launches += 2;
+            tr.e->tlaunch[0] += 2;
+        }
+        for (const FftScale &fs : dft_scales) {
+            DftArgs d;
+            d.src = rows.src;
+            d.frame_stride = frame_stride;
+            d.row_pitch = row_pitch;
+            d.bpp = e->bpp;
+            d.pixmode = e->pixmode;
+            d.x_off = x_off;
+            d.y_off = y_off;
+            d.ring = e->ring;
+            d.E = e->E;
+            d.first_label = first_label + f0;
+            d.R = e->R;
+            d.nframes = nf;
+            d.sc = fs;
+            d.tables = e->dft_tab[fs.log2s - kDftMinLog2];
+            d.status = e->status_d;
+            const long long tiles = 1LL << (2 * fs.log2side), tpb = 128 / fs.s;
+            const long long items = (tiles + tpb - 1) / tpb * nf;
+            const unsigned grid = static_cast<unsigned>(std::min<long long>(items, e->sms));
+            switch (fs.log2s) {
+                case 5: dft_bf16_kernel<5><<<grid, kDftThreads, dft_smem_bytes(32), e->fft_stream>>>(d); break;
+                case 6: dft_bf16_kernel<6><<<grid, kDftThreads, dft_smem_bytes(64), e->fft_stream>>>(d); break;
+                default: dft_bf16_kernel<7><<<grid, kDftThreads, dft_smem_bytes(128), e->fft_stream>>>(d); break;
+            }
+            CUDA_TRY(cudaGetLastError());
+            e->launches += 1;
+            tr.e->tlaunch[0] += 1;
+        }
         // the ROI's pixels read once and the frame's spectra written once
         e->tbytes[0] += static_cast<double>(nf) *
                         (static_cast<double>(e->M) * e->M * e->bpp + static_cast<double>(frame_bytes));
@@ -387,23 +434,28 @@ int launch_lag(ddm_engine *e, const Launch &L) {
     }
     e->tab_used[ts] = true;
 
-    const unsigned blocks = static_cast<unsigned>((e->E + lag_cta_elems(J) - 1) / lag_cta_elems(J));
-    const size_t smem = lag_smem_bytes(J, ntab);
+    const int G = J <= 32 ? e->lag_geom : 0;
+    const unsigned blocks = static_cast<unsigned>((e->E + lag_cta_elems(J, G) - 1) / lag_cta_elems(J, G));
+    const size_t smem = lag_smem_bytes(J, ntab, G);
     if (e->defer_lag) {  // a server issues it with other engines' work in one launch
         e->deferred.push_back(DeferredLag{J, td, blocks, smem});
         return DDM_OK;
     }
     TimedRange tr(e, 1);
     // persistent grid: every resident CTA walks element blocks blockIdx.x, + gridDim.x, ...
-    const unsigned grid = std::min<unsigned>(blocks, static_cast<unsigned>(kLagCtasPerSm * e->sms));
-    switch (J) {
-#define LAG_CASE(JJ)                                                                                   \
-    case JJ:                                                                                           \
-        lag_pipe_kernel<JJ><<<grid, kLagThreads, smem, e->stream>>>(e->ring, e->acc, e->E, td, e->status_d, \
-                                                                     e->maps, static_cast<int>(blocks),  \
-                                                                     e->wait_cycles);                    \
+    const unsigned grid = std::min<unsigned>(blocks, static_cast<unsigned>(lag_ctas_per_sm(G) * e->sms));
+    switch (J * kLagGeoms + G) {
+#define LAG_CASE(JJ, GG)                                                                                     \
+    case JJ * kLagGeoms + GG:                                                                                \
+        lag_pipe_kernel<JJ, GG><<<grid, lag_threads(GG), smem, e->stream>>>(e->ring, e->acc, e->E, td,      \
+                                                                           e->status_d, e->maps,             \
+                                                                           static_cast<int>(blocks),         \
+                                                                           e->wait_cycles);                  \
         break;
-        LAG_CASE(4) LAG_CASE(8) LAG_CASE(16) LAG_CASE(20) LAG_CASE(24) LAG_CASE(30) LAG_CASE(32) LAG_CASE(64)
+        LAG_CASE(4, 0) LAG_CASE(8, 0) LAG_CASE(16, 0) LAG_CASE(20, 0) LAG_CASE(24, 0) LAG_CASE(30, 0)
+        LAG_CASE(32, 0) LAG_CASE(64, 0)
+        LAG_CASE(4, 1) LAG_CASE(8, 1) LAG_CASE(16, 1) LAG_CASE(20, 1) LAG_CASE(24, 1) LAG_CASE(30, 1)
+        LAG_CASE(32, 1)
 #undef LAG_CASE
         default: return fail(DDM_ERR_STATE, "internal: no lag kernel for this frame count");
     }
@@ -428,8 +480,9 @@ int check_device_status(ddm_engine *e) {
     int st = 0;
     CUDA_TRY(cudaMemcpyAsync(&st, e->status_d, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
     CUDA_TRY(cudaStreamSynchronize(e->stream));
-    if (st != 0) return fail(DDM_ERR_CUDA, "a lag-kernel pipeline wait timed out (device status " +
-                                               std::to_string(st) + "); results are incomplete");
+    if (st != 0) return fail(DDM_ERR_CUDA, std::string(st == 2 ? "a tensor-core DFT wait" : "a lag-kernel pipeline wait") +
+                                               " timed out (device status " + std::to_string(st) +
+                                               "); results are incomplete");
     return DDM_OK;
 }
 
@@ -629,6 +682,12 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
     e->multistream = cfg->multistream ? 1 : 0;
     e->N = cfg->total_frames;
     e->G = cfg->dump_every;
+    e->lag_geom = cfg->lag_geometry ? 1 : 0;
+    if (cfg->fft_group_frames < 0) {
+        delete e;
+        return fail(DDM_ERR_INVALID_ARG, "fft_group_frames must be >= 0");
+    }
+    e->fft_group = cfg->fft_group_frames;
     e->device = cfg->device;
     const bool compat = e->estimator == DDM_EST_COMPAT;
 
@@ -681,9 +740,15 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
     if (cfg->lag_batch_frames < -1 || cfg->lag_batch_frames > kMaxJ)
         return bail(fail(DDM_ERR_INVALID_ARG, "lag_batch_frames must be -1.." + std::to_string(kMaxJ)));
     int lag_batch_cfg = cfg->lag_batch_frames;
-    if (lag_batch_cfg == -1) {  // the tuned value for this shape, if a cache names one
-        int tuned = 0;
-        lag_batch_cfg = tune_lookup(std::getenv("DDM_TUNE_CACHE"), tune_key(cfg), &tuned, nullptr) ? tuned : 0;
+    if (lag_batch_cfg == -1) {  // the tuned values for this shape, if a cache names them
+        TunedValues tv;
+        if (tune_lookup(std::getenv("DDM_TUNE_CACHE"), tune_key(cfg), &tv)) {
+            lag_batch_cfg = tv.lag_batch;
+            e->lag_geom = tv.lag_geometry;
+            e->fft_group = tv.fft_group;
+        } else {
+            lag_batch_cfg = 0;
+        }
     }
     // default: unbiased launches of kPieceFrames (32) frames, the instantiated register-frame
     // count the kernel's cost per launch is set by (32 frames take about the time of 30);
@@ -782,6 +847,17 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
 
     // FFT twiddle tables (FP64 math rounded to FP32), one per transform length
     {
+        e->small_dft = cfg->small_tile_dft != 0;
+        if (e->small_dft)
+            for (int s : e->scales) {
+                const int l = log2i(s);
+                if (l < kDftMinLog2 || l > kDftMaxLog2 || e->dft_tab[l - kDftMinLog2]) continue;
+                const std::vector<uint16_t> t = dft_tables(s);
+                uint4 **dst = &e->dft_tab[l - kDftMinLog2];
+                if ((st = dev_alloc(e, dst, t.size() * 2 / sizeof(uint4)))) return bail(st);
+                if (cudaMemcpy(*dst, t.data(), t.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess)
+                    return bail(fail(DDM_ERR_CUDA, "DFT table upload failed"));
+            }
         std::vector<float2> tw = fft_twiddle_tables(e->M);
         if ((st = dev_alloc(e, &e->tw, tw.size()))) return bail(st);
         if (cudaMemcpy(e->tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice) != cudaSuccess)
@@ -844,7 +920,17 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
         cudaFuncSetAttribute(lag_pipe_kernel<24>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
         cudaFuncSetAttribute(lag_pipe_kernel<30>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
         cudaFuncSetAttribute(lag_pipe_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
-        cudaFuncSetAttribute(lag_pipe_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess)
+        cudaFuncSetAttribute(lag_pipe_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
+        cudaFuncSetAttribute(lag_pipe_kernel<4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
+        cudaFuncSetAttribute(lag_pipe_kernel<8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
+        cudaFuncSetAttribute(lag_pipe_kernel<16, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
+        cudaFuncSetAttribute(lag_pipe_kernel<20, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
+        cudaFuncSetAttribute(lag_pipe_kernel<24, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
+        cudaFuncSetAttribute(lag_pipe_kernel<30, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
+        cudaFuncSetAttribute(lag_pipe_kernel<32, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
+        cudaFuncSetAttribute(dft_bf16_kernel<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, dft_smem_bytes(32)) != cudaSuccess ||
+        cudaFuncSetAttribute(dft_bf16_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, dft_smem_bytes(64)) != cudaSuccess ||
+        cudaFuncSetAttribute(dft_bf16_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, dft_smem_bytes(128)) != cudaSuccess)
         return bail(fail(DDM_ERR_CUDA, "cudaFuncSetAttribute failed"));
 
     // Zero the accumulators on the engine's private FFT stream, ahead of its first FFT: every
@@ -1255,6 +1341,8 @@ extern "C" int ddm_get_info(const ddm_engine *e, ddm_info *info) {
     info->stream = e->stream;
     info->frames_needed = e->estimator == DDM_EST_COMPAT ? e->frames_read : 0;
     info->lag_batch_frames = e->lag_batch;
+    info->lag_geometry = e->lag_geom;
+    info->fft_group_frames = e->fft_group;
     return DDM_OK;
 }
 

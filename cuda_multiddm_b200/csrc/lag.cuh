@@ -52,6 +52,15 @@ namespace ddm {
 constexpr int kLagConsumerWarps = 4;
 constexpr int kLagThreads = kLagConsumerWarps * 32 + 32;  // consumers + one producer warp
 constexpr int kLagCtasPerSm = 3;  // registers (128 a thread) and shared memory (~70 KB a CTA) both allow 3
+// Geometries of the kernel (template parameter G): 0 "narrow", the layout above -- one
+// consumer thread per element holding all J <= 32 register frames, four consumer warps, three
+// CTAs per SM; 1 "wide" -- two lanes per element holding J/2 frames each (a warp's partner
+// load then reads 16 elements, one shared-memory wavefront for 32 pairs), eight consumer warps
+// over the same 128-element block, two CTAs per SM (16 consumer warps per SM instead of 12).
+constexpr int kLagGeoms = 2;
+__host__ __device__ constexpr int lag_cwarps(int G) { return G ? 8 : kLagConsumerWarps; }
+__host__ __device__ constexpr int lag_threads(int G) { return (lag_cwarps(G) + 1) * 32; }
+__host__ __device__ constexpr int lag_ctas_per_sm(int G) { return G ? 2 : kLagCtasPerSm; }
 constexpr int kLagSmemMax = 220 * 1024;
 // Register-frame counts the kernel is instantiated for (a launch uses the smallest >= nreg).
 constexpr int kLagJs[] = {4, 8, 16, 20, 24, 30, 32, 64};
@@ -78,9 +87,11 @@ constexpr int kLagFullFlag = 1, kLagRunFlag = 2;
 // block is therefore 128 or 64 elements and a ring slot 1 KB or 512 B. The ring must hold a
 // window plus its alignment, ceil((J - 1) / kLagGroup) + 1 groups, with room to read ahead:
 // 64 slots (8 groups) up to 32 frames, 128 slots (16 groups) for 64; both are 64 KB.
-__host__ __device__ constexpr int lag_lanes(int J) { return J > 32 ? 2 : 1; }
-__host__ __device__ constexpr int lag_cta_elems(int J) { return kLagConsumerWarps * 32 / lag_lanes(J); }
-__host__ __device__ constexpr uint32_t lag_slot_bytes(int J) { return lag_cta_elems(J) * 8u; }
+__host__ __device__ constexpr int lag_lanes(int J, int G = 0) { return (J > 32 || G) ? 2 : 1; }
+__host__ __device__ constexpr int lag_cta_elems(int J, int G = 0) { return lag_cwarps(G) * 32 / lag_lanes(J, G); }
+__host__ __device__ constexpr uint32_t lag_slot_bytes(int J, int G = 0) { return lag_cta_elems(J, G) * 8u; }
+// tensor-map box width index (LagMaps::box[w]): 128-element blocks 0, 64-element blocks 1
+__host__ __device__ constexpr int lag_map_index(int J, int G = 0) { return lag_cta_elems(J, G) == 128 ? 0 : 1; }
 __host__ __device__ constexpr int lag_ring_slots(int J) { return J > 32 ? 128 : 64; }
 __host__ __device__ constexpr int lag_group_slots(int J) { return lag_ring_slots(J) / kLagGroup; }
 
@@ -190,15 +201,17 @@ struct LagMaps {
 // (n * ngroups * kLagGroup + u) % lag_ring_slots(J). Neither side
 // ever waits for the whole CTA. The CTA handles element blocks block_begin, + block_step, ...
 // below block_end; `maps` may live in kernel parameter space or global memory.
-template <int J>
+template <int J, int G = 0>
 __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, float2 *__restrict__ acc, long long E,
                                               const int *__restrict__ table, int *__restrict__ status,
                                               const LagMaps &maps, int block_begin, int block_end, int block_step,
                                               long long wait_cycles) {
-    constexpr int kLanes = lag_lanes(J);
+    constexpr int kLanes = lag_lanes(J, G);
     constexpr int kJT = J / kLanes;  // register frames per thread
-    constexpr int kElems = lag_cta_elems(J);
-    constexpr uint32_t kSlotBytes = lag_slot_bytes(J);
+    constexpr int kElems = lag_cta_elems(J, G);
+    constexpr int kCW = lag_cwarps(G);  // consumer warps; warp kCW produces
+    constexpr int kThreads = lag_threads(G);
+    constexpr uint32_t kSlotBytes = lag_slot_bytes(J, G);
     constexpr int kSlots = lag_ring_slots(J);
     constexpr int kGS = lag_group_slots(J);
     constexpr uint32_t kRingBytes = kSlots * kSlotBytes;
@@ -215,11 +228,11 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     const int ntab = lag_table_ints(table[kTabNtau], table[kTabNunion], table[kTabNgroups], table[kTabNruns]);
-    for (int i = tid; i < ntab; i += kLagThreads) tab[i] = table[i];
+    for (int i = tid; i < ntab; i += kThreads) tab[i] = table[i];
     if (tid == 0) {
         for (int i = 0; i < kGS; i++) {
             mbar_init(&full[i], 1);
-            mbar_init(&empty[i], kLagConsumerWarps);
+            mbar_init(&empty[i], kCW);
         }
         *abort_flag = 0;
         *issued = 0;
@@ -236,7 +249,7 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
     const int *gptr = uslot + nu;
     const int *runs = gptr + ngroups + 1;
 
-    if (warp == kLagConsumerWarps) {
+    if (warp == kCW) {
         // ---------------- producer: running group G is fill G / kGS of group slot G % kGS
         if (lane == 0 && ngroups > 0) {
             // group g of the CTA's element block `block`
@@ -259,7 +272,7 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
                     for (int r = r0; r < r1; r++) {
                         const int run = runs[r];
                         tma_load_2d(smem + (gs * kLagGroup + lag_run_rel(run)) * kSlotBytes,
-                                    &maps.box[kLanes - 1][lag_run_log2rows(run)], static_cast<int>(e0),
+                                    &maps.box[lag_map_index(J, G)][lag_run_log2rows(run)], static_cast<int>(e0),
                                     lag_run_slot(run), &full[gs]);
                     }
                 }
@@ -440,13 +453,13 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
 }
 
 // One engine's launch: CTA b handles element blocks b, b + gridDim.x, ... below nblocks.
-template <int J>
-__global__ void __launch_bounds__(kLagThreads, kLagCtasPerSm)
+template <int J, int G = 0>
+__global__ void __launch_bounds__(lag_threads(G), lag_ctas_per_sm(G))
     lag_pipe_kernel(const float2 *__restrict__ ring, float2 *__restrict__ acc, long long E,
                     const int *__restrict__ table, int *__restrict__ status, const __grid_constant__ LagMaps maps,
                     int nblocks, long long wait_cycles) {
-    lag_pipe_body<J>(ring, acc, E, table, status, maps, static_cast<int>(blockIdx.x), nblocks, static_cast<int>(gridDim.x),
-                     wait_cycles);
+    lag_pipe_body<J, G>(ring, acc, E, table, status, maps, static_cast<int>(blockIdx.x), nblocks,
+                        static_cast<int>(gridDim.x), wait_cycles);
 }
 
 // The lag work of several engines (served streams) in one launch: item i owns CTAs
@@ -479,8 +492,8 @@ __global__ void __launch_bounds__(kLagThreads, kLagCtasPerSm)
 
 // Dynamic shared memory of a launch of lag_pipe_kernel<J> with a table of table_ints ints
 // (1 KB of alignment slack, ring, barriers, abort flag, issued-group count, table).
-inline size_t lag_smem_bytes(int J, int table_ints) {
-    return 1024 + static_cast<size_t>(lag_ring_slots(J)) * lag_slot_bytes(J) + 2 * sizeof(uint64_t) * lag_group_slots(J) +
+inline size_t lag_smem_bytes(int J, int table_ints, int G = 0) {
+    return 1024 + static_cast<size_t>(lag_ring_slots(J)) * lag_slot_bytes(J, G) + 2 * sizeof(uint64_t) * lag_group_slots(J) +
            sizeof(int) * (2 + table_ints);
 }
 

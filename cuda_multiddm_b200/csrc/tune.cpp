@@ -1,12 +1,17 @@
-// Autotuner for the lag blocking: the number of frames one lag launch pairs
-// (ddm_config.lag_batch_frames). A launch pairs its J register frames against the union of
-// their partner frames, so larger J reads fewer partner bytes per frame, but J above the
-// ingest piece holds frames back, and the kernel's per-element cost changes with J (one or
-// two lanes per element, ring and window sizes): the best J depends on the frame size,
-// scales, tau list and chunk. ddm_autotune times the candidates on the caller's shape with
-// synthetic frames resident on the device (the engine's steady state: every timed frame has
-// all its lags) and keeps the winner in a JSON cache keyed by the shape, one key per line;
-// engines opened with lag_batch_frames = -1 look their shape up in the cache named by the
+// Autotuner for the engine's blocking choices:
+//   lag_batch_frames  the frames one lag launch pairs. A launch pairs its J register frames
+//                     against the union of their partner frames, so larger J reads fewer
+//                     partner bytes per frame, but J above the ingest piece holds frames back,
+//                     and the kernel's per-element cost changes with J;
+//   lag_geometry      one thread per element (4 consumer warps, 3 CTAs per SM) or two
+//                     (8 consumer warps, 2 CTAs per SM): occupancy against per-entry overhead;
+//   fft_group_frames  frames per FFT launch: fewer, larger launches against keeping the row
+//                     pass's output in L2 and overlapping host copies with the FFT.
+// The best values depend on the frame size, scales, tau list and chunk. ddm_autotune times the
+// (J, geometry) candidates, then the FFT groups with the fastest of those, on the caller's
+// shape with synthetic frames resident on the device (the engine's steady state: every timed
+// frame has all its lags), and keeps the winner in a JSON cache keyed by the shape, one key per
+// line; engines opened with lag_batch_frames = -1 look their shape up in the cache named by the
 // DDM_TUNE_CACHE environment variable.
 #include "tune.hpp"
 
@@ -38,6 +43,7 @@ uint64_t fnv1a(const std::vector<int> &v) {
 }
 
 const int kCandidates[] = {16, 24, 30, 32, 64};
+const int kFftGroups[] = {0, 4, 8, 16};
 
 }  // namespace
 
@@ -53,25 +59,36 @@ std::string tune_key(const ddm_config *cfg) {
     std::snprintf(hash, sizeof(hash), "%016llx", static_cast<unsigned long long>(fnv1a(taus)));
     k << "|t" << taus.size() << ":" << (taus.empty() ? 0 : taus.back()) << ":" << hash << "|c" << cfg->chunk_frames
       << "|e" << cfg->estimator;
+    if (cfg->small_tile_dft) k << "|dft";
     return k.str();
 }
 
-bool tune_lookup(const char *path, const std::string &key, int *lag_batch, double *fps) {
+bool tune_lookup(const char *path, const std::string &key, TunedValues *out) {
     if (!path || !*path) return false;
     std::ifstream in(path);
     if (!in) return false;
     const std::string head = "\"" + key + "\": {";
     std::string line;
+    // the value after "name": within this shape's line (-1 when absent)
+    auto field = [&](size_t from, const char *name, double *v) {
+        const std::string n = std::string("\"") + name + "\": ";
+        const size_t a = line.find(n, from);
+        if (a == std::string::npos) return false;
+        *v = std::atof(line.c_str() + a + n.size());
+        return true;
+    };
     while (std::getline(in, line)) {
         const size_t p = line.find(head);
         if (p == std::string::npos) continue;
-        const size_t a = line.find("\"lag_batch_frames\": ", p);
-        const size_t b = line.find("\"frames_per_s\": ", p);
-        if (a == std::string::npos) return false;
-        const int v = std::atoi(line.c_str() + a + 20);
-        if (v < 1 || v > 64) return false;
-        *lag_batch = v;
-        if (fps) *fps = b == std::string::npos ? 0.0 : std::atof(line.c_str() + b + 16);
+        double J = 0, G = 0, F = 0, fps = 0;
+        if (!field(p, "lag_batch_frames", &J) || J < 1 || J > 64) return false;
+        field(p, "lag_geometry", &G);  // absent in caches written before the geometry was tuned: 0
+        field(p, "fft_group_frames", &F);
+        field(p, "frames_per_s", &fps);
+        out->lag_batch = static_cast<int>(J);
+        out->lag_geometry = (G == 1 && J <= 32) ? 1 : 0;
+        out->fft_group = F > 0 ? static_cast<int>(F) : 0;
+        out->fps = fps;
         return true;
     }
     return false;
@@ -106,11 +123,15 @@ bool tune_store(const char *path, const std::string &key, const std::string &ent
     return std::rename(tmp.c_str(), path) == 0;
 }
 
-// Frames/s of one engine with lag_batch_frames = J on `frames` (device memory): pre-roll until
+// Frames/s of one engine with lag_batch_frames = J, lag_geometry = G and fft_group_frames = F
+// on `frames` (device memory): pre-roll until
 // every frame has all its lags, then `timed` chunks between two synchronisations.
-int time_candidate(const ddm_config &base, int J, const uint8_t *frames, int n_frames, int timed, double *fps) {
+int time_candidate(const ddm_config &base, int J, int G, int F, const uint8_t *frames, int n_frames, int timed,
+                   double *fps) {
     ddm_config c = base;
     c.lag_batch_frames = J;
+    c.lag_geometry = G;
+    c.fft_group_frames = F;
     c.dump_every = 0;
     ddm_engine *e = nullptr;
     int st = ddm_open(&c, &e);
@@ -174,7 +195,12 @@ extern "C" int ddm_autotune(const ddm_config *cfg, const char *cache_path, ddm_t
         return fail(DDM_ERR_INVALID_ARG, "ddm_autotune: the lag blocking is tuned for the unbiased estimator");
     const std::string key = tune_key(cfg);
     *out = ddm_tuning{};
-    if (tune_lookup(cache_path, key, &out->lag_batch_frames, &out->frames_per_s)) {
+    TunedValues tv;
+    if (tune_lookup(cache_path, key, &tv)) {
+        out->lag_batch_frames = tv.lag_batch;
+        out->lag_geometry = tv.lag_geometry;
+        out->fft_group_frames = tv.fft_group;
+        out->frames_per_s = tv.fps;
         out->from_cache = 1;
         return DDM_OK;
     }
@@ -200,30 +226,42 @@ extern "C" int ddm_autotune(const ddm_config *cfg, const char *cache_path, ddm_t
     cands.erase(std::unique(cands.begin(), cands.end()), cands.end());
     const int timed = std::max(4, (8 * 30 + cfg->chunk_frames - 1) / cfg->chunk_frames);
     std::ostringstream tried;
-    int best = 0, first_error = DDM_OK;
+    int best = 0, best_g = 0, best_f = 0, first_error = DDM_OK;
     std::string first_message;
     double best_fps = 0.0;
-    for (int J : cands) {  // a candidate that cannot run here (e.g. its ring does not fit) is skipped
+    // a candidate that cannot run here (e.g. its ring does not fit) is skipped
+    auto run = [&](int J, int G, int F) {
         double fps = 0.0;
-        const int st = time_candidate(*cfg, J, dev, n_frames, timed, &fps);
+        const int st = time_candidate(*cfg, J, G, F, dev, n_frames, timed, &fps);
         if (st) {
             if (!first_error) first_error = st, first_message = last_error();
-            continue;
+            return;
         }
         char buf[64];
-        std::snprintf(buf, sizeof(buf), "%s\"%d\": %.1f", tried.tellp() > 0 ? ", " : "", J, fps);
+        std::snprintf(buf, sizeof(buf), "%s\"%d/%d/%d\": %.1f", tried.tellp() > 0 ? ", " : "", J, G, F, fps);
         tried << buf;
-        if (fps > best_fps) best_fps = fps, best = J;
+        if (fps > best_fps) best_fps = fps, best = J, best_g = G, best_f = F;
+    };
+    for (int J : cands)
+        for (int G = 0; G < (J <= 32 ? 2 : 1); G++) run(J, G, 0);
+    if (best > 0) {
+        const int J = best, G = best_g;
+        for (int F : kFftGroups)
+            if (F > 0) run(J, G, F);
     }
     cudaFree(dev);
     if (best == 0) return fail(first_error ? first_error : DDM_ERR_CUDA, "ddm_autotune: no candidate ran: " + first_message);
     out->lag_batch_frames = best;
+    out->lag_geometry = best_g;
+    out->fft_group_frames = best_f;
     out->frames_per_s = best_fps;
     out->from_cache = 0;
     if (cache_path && *cache_path) {
-        char buf[96];
-        std::snprintf(buf, sizeof(buf), "{\"lag_batch_frames\": %d, \"frames_per_s\": %.1f, \"candidates\": {", best,
-                      best_fps);
+        char buf[192];
+        std::snprintf(buf, sizeof(buf),
+                      "{\"lag_batch_frames\": %d, \"lag_geometry\": %d, \"fft_group_frames\": %d, "
+                      "\"frames_per_s\": %.1f, \"candidates\": {",
+                      best, best_g, best_f, best_fps);
         if (!tune_store(cache_path, key, std::string(buf) + tried.str() + "}}"))
             return fail(DDM_ERR_INVALID_ARG, std::string("ddm_autotune: cannot write the cache ") + cache_path);
     }

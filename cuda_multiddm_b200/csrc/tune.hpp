@@ -1,4 +1,4 @@
-// Lag-blocking autotuner: shape keys and the JSON cache (tune.cpp).
+// Autotuner: shape keys and the JSON cache (tune.cpp).
 #pragma once
 
 #include <string>
@@ -8,9 +8,13 @@
 namespace ddm {
 
 // Key of cfg's shape: frame size and depth, scales, tau list (count, largest, FNV-1a hash),
-// chunk and estimator.
+// chunk, estimator and the small-tile DFT choice.
 std::string tune_key(const ddm_config *cfg);
-// The lag_batch_frames (and frames/s) cached for `key` in the file at `path`, if any.
-bool tune_lookup(const char *path, const std::string &key, int *lag_batch, double *fps);
+// The tuned values cached for `key` in the file at `path`, if any.
+struct TunedValues {
+    int lag_batch = 0, lag_geometry = 0, fft_group = 0;
+    double fps = 0.0;
+};
+bool tune_lookup(const char *path, const std::string &key, TunedValues *out);
 
 }  // namespace ddm

@@ -35,6 +35,9 @@ class EngineConfig:
     stream: int | None = None          # a cudaStream_t as an integer, or None
     lag_batch_frames: int = 0          # frames per lag launch (1..64; 0 = 32 unbiased, min(chunk_frames, 32) compat;
                                        # -1 = the value autotune() cached for this shape in $DDM_TUNE_CACHE)
+    small_tile_dft: bool = False       # split-BF16 tensor-core DFT for tiles of side 32..128
+    lag_geometry: int = 0              # lag kernel: 0 one thread per element, 1 two threads per element
+    fft_group_frames: int = 0          # frames per FFT launch (0 = as many as 256 MB of spectra hold)
     _keep: list = field(default_factory=list, repr=False)
 
     def to_c(self) -> Config:
@@ -48,7 +51,8 @@ class EngineConfig:
                       self.y_offset, sc, len(self.scales), ta, len(self.taus), la, len(self.lambdas),
                       C.c_float(self.tolerance), self.chunk_frames, est, int(bool(self.multistream)),
                       self.total_frames, self.dump_every, self.hbm_budget_bytes, self.device,
-                      C.c_void_p(self.stream) if self.stream else None, self.lag_batch_frames)
+                      C.c_void_p(self.stream) if self.stream else None, self.lag_batch_frames,
+                      int(bool(self.small_tile_dft)), int(self.lag_geometry), int(self.fft_group_frames))
 
 
 def tune_key(cfg: EngineConfig) -> str:
@@ -61,15 +65,17 @@ def tune_key(cfg: EngineConfig) -> str:
 
 
 def autotune(cfg: EngineConfig, cache: str | None = None) -> dict:
-    """Time lag_batch_frames candidates on cfg's shape (unbiased estimator) and return
-    {"lag_batch_frames", "frames_per_s", "from_cache"}; with `cache`, look the shape up there
+    """Time the lag blocking x lag-kernel geometry candidates, then the FFT launch groups, on
+    cfg's shape (unbiased estimator) and return {"lag_batch_frames", "lag_geometry",
+    "fft_group_frames", "frames_per_s", "from_cache"}; with `cache`, look the shape up there
     first and store the result afterwards (engines opened with lag_batch_frames = -1 and
     DDM_TUNE_CACHE set to that file use it)."""
     from ._lib import Tuning
     c = cfg.to_c()
     t = Tuning()
     check(lib().ddm_autotune(C.byref(c), cache.encode() if cache else None, C.byref(t)))
-    return {"lag_batch_frames": t.lag_batch_frames, "frames_per_s": t.frames_per_s, "from_cache": bool(t.from_cache)}
+    return {"lag_batch_frames": t.lag_batch_frames, "lag_geometry": t.lag_geometry,
+            "fft_group_frames": t.fft_group_frames, "frames_per_s": t.frames_per_s, "from_cache": bool(t.from_cache)}
 
 
 def isf_blocks(isf: np.ndarray, scales: Sequence[int], n_lambda: int, n_tau: int) -> dict:

@@ -81,6 +81,22 @@ typedef struct {
                                       (0 = min(C, 32)): A-frames per launch. -1: the value
                                       ddm_autotune cached for this shape in the file named by
                                       the DDM_TUNE_CACHE environment variable, else as 0. */
+    int small_tile_dft;            /* 1: tiles of side 32, 64 and 128 are transformed by the
+                                      split-BF16 tensor-core DFT (BF16 hi/lo operands, FP32
+                                      accumulation; spectra within ~1e-5 of the tile maximum,
+                                      ISF within 1e-3) instead of the FP32 FFT; 0: FP32 FFT for
+                                      every scale (the reference uses cuFFT in FP32 for all,
+                                      src/DDM.cu:648-677). Other scales always use the FP32 FFT. */
+    int lag_geometry;              /* lag-kernel geometry for launches of up to 32 frames:
+                                      0 = one thread per spectrum element, four consumer warps
+                                      and three CTAs per SM; 1 = two threads per element (half
+                                      the frames each), eight consumer warps and two CTAs per SM.
+                                      The same pairs, their FP32 sums formed in another order
+                                      (both within 1e-5 of the FP64 oracle). With
+                                      lag_batch_frames = -1 the tuned geometry is used. */
+    int fft_group_frames;          /* frames per FFT launch (both passes over every scale);
+                                      0 = as many as 256 MB of spectra hold (at least 1). With
+                                      lag_batch_frames = -1 the tuned value is used. */
 } ddm_config;
 
 typedef struct ddm_engine ddm_engine;
@@ -134,18 +150,25 @@ int ddm_finalize_async(ddm_engine *e, double *isf_out, long capacity);
  * a kernel queued before it reported a failure (the status ddm_finalize checks). */
 int ddm_wait_isf(ddm_engine *e);
 
-/* Lag-blocking autotuner (the reference has none; its work is one launch per (scale, tau,
- * frame)). ddm_autotune times lag_batch_frames = 16, 24, 30, 32, 64 and the chunk size on
- * cfg's shape (unbiased estimator only) with synthetic frames on the device, in the engine's
- * steady state, and returns the fastest; with a cache path it first looks the shape up
- * there and afterwards stores the result (a JSON object, one shape key per line, with the
- * frames/s of every candidate). ddm_tune_key writes the shape key (frame size and depth,
- * scales, tau count / largest / hash, chunk, estimator) into out (capacity bytes, NUL
+/* Autotuner (the reference has none: its block sizes are constants, src/constants.hpp:11-13,
+ * and its lag work is one launch per (scale, tau, frame)). ddm_autotune times, on cfg's shape
+ * (unbiased estimator only) with synthetic frames on the device in the engine's steady state,
+ * first every lag blocking lag_batch_frames in {16, 24, 30, 32, 64, chunk} with each lag-kernel
+ * geometry (lag_geometry 0 and 1; 64 frames run geometry 0 only), then, with the fastest of
+ * those, the FFT launch group fft_group_frames in {0 (256 MB of spectra), 4, 8, 16} frames,
+ * and returns the fastest combination; with a cache path it first looks the shape up there and
+ * afterwards stores the result (a JSON object, one shape key per line, with the frames/s of
+ * every candidate as "J/G/F"). Engines opened with lag_batch_frames = -1 take all three tuned
+ * values. cfg's small_tile_dft is kept as given (it changes the precision, so it is never
+ * chosen by timing). ddm_tune_key writes the shape key (frame size and depth, scales, tau
+ * count / largest / hash, chunk, estimator, small_tile_dft) into out (capacity bytes, NUL
  * terminated) and returns its length, or -1. */
 typedef struct {
     int lag_batch_frames;
     double frames_per_s;   /* of the winner, as timed (or as cached) */
     int from_cache;        /* 1: found in the cache, nothing timed */
+    int lag_geometry;      /* the winner's lag-kernel geometry */
+    int fft_group_frames;  /* the winner's FFT launch group (0 = the 256 MB rule) */
 } ddm_tuning;
 int ddm_autotune(const ddm_config *cfg, const char *cache_path, ddm_tuning *out);
 long ddm_tune_key(const ddm_config *cfg, char *out, long capacity);
@@ -229,6 +252,8 @@ typedef struct {
     void *stream;
     long frames_needed;
     int lag_batch_frames;          /* frames per lag launch in use (after defaults / tuning) */
+    int lag_geometry;              /* lag-kernel geometry in use */
+    int fft_group_frames;          /* frames per FFT launch in use */
 } ddm_info;
 int ddm_get_info(const ddm_engine *e, ddm_info *info);
 

@@ -367,3 +367,25 @@ def test_wait_timeout_is_reported_and_device_stays_usable():
         got = eng.isf()
     want, _ = O.ddm_run(frames, scales, taus, lambdas, estimator=O.EST_UNBIASED, chunk=10)
     assert_isf_close(got, want, scales, len(lambdas), len(taus))
+
+
+@pytest.mark.parametrize("lag_batch", [16, 30, 32])
+def test_wide_lag_geometry_matches_oracle(lag_batch):
+    """The two-threads-per-element lag kernel (lag_geometry = 1) on a multi-scale, multi-tile
+    case whose element blocks outnumber the persistent grid's CTAs, with fused tau runs, against
+    the FP64 oracle; and against the one-thread-per-element kernel within FP32 rounding."""
+    frames = media.synth_video(91, 512, 512, 70, 600, step_var=1.0)
+    scales, taus = [512, 256, 128], [1, 2, 3, 4, 5, 6, 7, 8, 11, 17, 26, 40]
+    lambdas = media.log_lambdas(2, 256, 9)
+    want, _ = O.ddm_run(frames, scales, taus, lambdas, estimator=O.EST_UNBIASED, chunk=10)
+    got = {}
+    for geom in (0, 1):
+        cfg = EngineConfig(frame_width=512, frame_height=512, scales=scales, taus=taus, lambdas=lambdas,
+                           chunk_frames=10, estimator="unbiased", lag_batch_frames=lag_batch, lag_geometry=geom)
+        with Engine(cfg) as eng:
+            eng.submit(frames)
+            eng.finalize()
+            got[geom] = eng.isf()
+        assert_isf_close(got[geom], want, scales, len(lambdas), len(taus))
+    rel = np.abs(got[1] - got[0]) / np.maximum(np.abs(got[0]), 1e-9 * np.abs(got[0]).max())
+    assert float(rel.max()) <= 2e-6

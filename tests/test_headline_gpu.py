@@ -4,7 +4,8 @@ log-spaced 1..500, 30 lambdas log-spaced 2..512, 30-frame chunks, unbiased estim
 through the C ABI exactly as the benchmark runs it -- 32-frame lag launches over a 591-slot
 ring, a union of about 496 partner frames per launch, unfused entries for the larger taus,
 the persistent grid walking every element block -- and again with 64-frame launches, and
-both are compared with one FP64 oracle run.
+both are compared with one FP64 oracle run; the 32-frame launches run in both lag-kernel
+geometries (one thread per element, and two threads per element).
 
 Tolerance: 1e-5 relative per ISF bin (FP32 FFT and lag arithmetic with compensated
 accumulation, FP64 azimuthal reduction), with an absolute floor of 1e-9 of the largest
@@ -58,13 +59,13 @@ def per_bin_errors(got, want, scales, Q, T):
     return out, worst
 
 
-@pytest.mark.parametrize("lag_batch,ring", [(32, 591), (64, 623)])
-def test_headline_configuration_matches_oracle(headline, lag_batch, ring):
+@pytest.mark.parametrize("lag_batch,ring,geometry", [(32, 591, 0), (64, 623, 0), (32, 591, 1)])
+def test_headline_configuration_matches_oracle(headline, lag_batch, ring, geometry):
     w, video, want = headline
     side = w["side"]
     cfg = EngineConfig(frame_width=side, frame_height=side, scales=w["scales"], taus=w["taus"],
                        lambdas=w["lambdas"], tolerance=1.2, chunk_frames=bench.CHUNK, estimator="unbiased",
-                       lag_batch_frames=lag_batch)
+                       lag_batch_frames=lag_batch, lag_geometry=geometry)
     with Engine(cfg) as eng:
         info = eng.info()
         assert info.ring_slots == ring and info.lag_batch_frames == lag_batch
@@ -78,7 +79,7 @@ def test_headline_configuration_matches_oracle(headline, lag_batch, ring):
     path = os.environ.get("DDM_PARITY_REPORT")
     if path:
         rep = json.loads(Path(path).read_text()) if Path(path).exists() else {}
-        rep[f"lag_batch_{lag_batch}"] = {
+        rep[f"lag_batch_{lag_batch}_geometry_{geometry}"] = {
             "worst": worst,
             "worst_per_scale": {str(s): float(e.max()) for s, e in errs.items()},
             "taus": list(w["taus"]), "lambdas": list(w["lambdas"]),

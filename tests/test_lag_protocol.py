@@ -209,7 +209,7 @@ def parity_done(completed: int, parity: int) -> bool:
 
 
 def replay(d: dict, seed: int, skip_empty_waits: bool = False, blocks: int = 1,
-           one_block_slots: bool = False) -> str:
+           one_block_slots: bool = False, consumers: int = CONSUMERS) -> str:
     """Random interleaving of the producer lane and the consumer warps, as lag_pipe_kernel
     walking ``blocks`` element blocks of one launch (its persistent grid): the producer issues
     group g of block n as running group G = n * ngroups + g into group slot G % slots; a
@@ -218,7 +218,9 @@ def replay(d: dict, seed: int, skip_empty_waits: bool = False, blocks: int = 1,
     the groups below the next window, and at the end of a block waits for and releases every
     group of the block. ``skip_empty_waits`` and ``one_block_slots`` plant errors the kernel
     avoids: not waiting on groups without frames, and looking for union entry u of every
-    block in the slot of group u // 8 (the rule for a single block)."""
+    block in the slot of group u // 8 (the rule for a single block). ``consumers`` is the
+    number of consumer warps: 4 in the one-thread-per-element geometry, 8 in the
+    two-threads-per-element one."""
     rnd = random.Random(seed)
     nreg, ntau, nu, ngroups, ub = d["nreg"], d["ntau"], d["nu"], d["ngroups"], d["ub"]
     gslots = ring_slots(pick_j(nreg)) // GROUP
@@ -226,7 +228,7 @@ def replay(d: dict, seed: int, skip_empty_waits: bool = False, blocks: int = 1,
     full_c, empty_c, empty_arr = [0] * gslots, [0] * gslots, [0] * gslots
     content = [None] * gslots  # which running group a group slot holds
     g_next = 0
-    warps = [{"b": 0, "e": 0, "waited": 0, "released": 0} for _ in range(CONSUMERS)]
+    warps = [{"b": 0, "e": 0, "waited": 0, "released": 0} for _ in range(consumers)]
 
     def landed(base: int, groups) -> bool:
         return all(parity_done(full_c[(base + g) % gslots], ((base + g) // gslots) & 1) for g in groups
@@ -236,14 +238,14 @@ def replay(d: dict, seed: int, skip_empty_waits: bool = False, blocks: int = 1,
         for g in range(s["released"], upto):
             gs = (base + g) % gslots
             empty_arr[gs] += 1
-            if empty_arr[gs] == CONSUMERS:
+            if empty_arr[gs] == consumers:
                 empty_arr[gs] = 0
                 empty_c[gs] += 1
         s["released"] = max(s["released"], upto)
 
     idle = 0
     while True:
-        actors = (["P"] if g_next < blocks * ngroups else []) + [w for w in range(CONSUMERS) if warps[w]["b"] < blocks]
+        actors = (["P"] if g_next < blocks * ngroups else []) + [w for w in range(consumers) if warps[w]["b"] < blocks]
         if not actors:
             return "ok"
         a = rnd.choice(actors)
@@ -293,6 +295,8 @@ def test_tables_and_protocol(probe):
         for seed in range(2):
             assert replay(d, seed) == "ok", (i, seed)
             assert replay(d, seed, blocks=3) == "ok", (i, seed)
+        if d["nreg"] <= 32:  # the two-threads-per-element geometry: eight consumer warps
+            assert replay(d, 0, blocks=3, consumers=8) == "ok", i
 
 
 def test_windows_must_ascend(probe):

@@ -1,6 +1,6 @@
-"""The lag-blocking autotuner (csrc/tune.cpp): shape keys (host only), and on the GPU the
-timing of the candidates, the JSON cache, engines that take the cached value with
-lag_batch_frames = -1, and the CLI's -U flag."""
+"""The autotuner (csrc/tune.cpp): shape keys (host only), and on the GPU the timing of the
+candidates (lag blocking x lag-kernel geometry, then FFT launch groups), the JSON cache,
+engines that take the cached values with lag_batch_frames = -1, and the CLI's -U flag."""
 import json
 import subprocess
 from pathlib import Path
@@ -13,6 +13,14 @@ from cuda_multiddm_b200 import DDMError, Engine, EngineConfig, autotune, media, 
 ROOT = Path(__file__).resolve().parents[1]
 CLI = ROOT / "cuda_multiddm_b200" / "ddm"
 CANDIDATES = {16, 24, 30, 32, 64}
+
+
+def candidate_keys(chunk: int, best_j: int, best_g: int) -> set:
+    """J/G/F keys the tuner times: every J with both geometries (64 with the first only) at
+    the default FFT group, then the winner's J/G with FFT groups of 4, 8 and 16 frames."""
+    js = CANDIDATES | {chunk}
+    keys = {f"{j}/{g}/0" for j in js for g in ((0, 1) if j <= 32 else (0,))}
+    return keys | {f"{best_j}/{best_g}/{f}" for f in (4, 8, 16)}
 
 
 def cfg(**kw):
@@ -31,6 +39,7 @@ def test_shape_key_names_the_shape_and_ignores_order():
     assert tune_key(cfg(chunk_frames=30)) != k
     assert tune_key(cfg(frame_width=256)) != k
     assert tune_key(cfg(lambdas=[2.0])) == k  # lambdas do not change the lag work
+    assert tune_key(cfg(small_tile_dft=True)) == k + "|dft"  # a precision choice, never tuned
 
 
 @pytest.mark.gpu
@@ -41,7 +50,13 @@ def test_autotune_times_caches_and_is_used(tmp_path, monkeypatch):
     assert first["frames_per_s"] > 0
     entry = json.loads(cache.read_text())[tune_key(cfg())]
     assert entry["lag_batch_frames"] == first["lag_batch_frames"]
-    assert set(entry["candidates"]) == {str(c) for c in CANDIDATES | {10}}
+    assert entry["lag_geometry"] == first["lag_geometry"] and entry["fft_group_frames"] == first["fft_group_frames"]
+    fps = entry["candidates"]
+    # the (J, geometry) winner of the first pass carried into the FFT-group pass
+    j0, g0 = max(((int(k.split("/")[0]), int(k.split("/")[1])) for k in fps if k.endswith("/0")),
+                 key=lambda jg: fps[f"{jg[0]}/{jg[1]}/0"])
+    assert set(fps) == candidate_keys(10, j0, g0)
+    assert entry["frames_per_s"] == pytest.approx(max(fps.values()), rel=1e-3)
     again = autotune(cfg(), str(cache))
     assert again["from_cache"] and again["lag_batch_frames"] == first["lag_batch_frames"]
     # a second shape goes in beside the first
@@ -52,11 +67,14 @@ def test_autotune_times_caches_and_is_used(tmp_path, monkeypatch):
     frames = media.synth_video(51, 128, 128, 60, 30, step_var=1.0)
     monkeypatch.setenv("DDM_TUNE_CACHE", str(cache))
     with Engine(cfg(lag_batch_frames=-1)) as eng:
-        assert eng.info().lag_batch_frames == first["lag_batch_frames"]
+        inf = eng.info()
+        assert inf.lag_batch_frames == first["lag_batch_frames"]
+        assert inf.lag_geometry == first["lag_geometry"] and inf.fft_group_frames == first["fft_group_frames"]
         eng.submit(frames)
         eng.finalize()
         auto = eng.isf()
-    with Engine(cfg(lag_batch_frames=first["lag_batch_frames"])) as eng:
+    with Engine(cfg(lag_batch_frames=first["lag_batch_frames"], lag_geometry=first["lag_geometry"],
+                    fft_group_frames=first["fft_group_frames"])) as eng:
         eng.submit(frames)
         eng.finalize()
         assert np.array_equal(eng.isf(), auto)
@@ -78,7 +96,7 @@ def test_cli_autotune_flag(tmp_path):
     r = subprocess.run([str(CLI), "-o", str(tmp_path / "a_"), *base, "-U", str(cache), "-v"], capture_output=True,
                        text=True, timeout=600)
     assert r.returncode == 0, r.stderr
-    assert "(timed)" in r.stderr and len(json.loads(cache.read_text())) == 1
+    assert "(timed)" in r.stderr and "lag_geometry" in r.stderr and len(json.loads(cache.read_text())) == 1
     r = subprocess.run([str(CLI), "-o", str(tmp_path / "b_"), *base, "-U", str(cache), "-v"], capture_output=True,
                        text=True, timeout=600)
     assert r.returncode == 0 and "(cached)" in r.stderr
