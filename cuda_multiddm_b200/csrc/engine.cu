@@ -109,6 +109,7 @@ struct ddm_engine {
     bool small_dft = false;
     int lag_geom = 0;  // lag-kernel geometry for launches of up to 32 frames (ddm_config.lag_geometry)
     int fft_group = 0;  // frames per FFT launch (ddm_config.fft_group_frames; 0 = the 256 MB rule)
+    int fft_two_pass = 0;  // 1: no per-tile kernel for tiles of side 32..128 (ddm_config.fft_two_pass)
     uint4 *dft_tab[kDftMaxLog2 - kDftMinLog2 + 1] = {nullptr, nullptr, nullptr};
     uint8_t *stage = nullptr;
     int *tables_d = nullptr, *tables_h = nullptr;
@@ -301,8 +302,9 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
     rows.R = e->R;
     rows.tw = e->tw;
     cols = rows;
-    int row_ctas = 0, col_ctas = 0, nfft = 0;
-    size_t smem = 0;
+    FftArgs tiles = rows;  // scales of side 32..128 through the per-tile kernel
+    int row_ctas = 0, col_ctas = 0, nfft = 0, tile_ctas = 0, ntile = 0;
+    size_t smem = 0, tile_smem = 0;
     std::vector<FftScale> dft_scales;  // scales for the tensor-core DFT
     for (int si = 0; si < e->S; si++) {
         const ScaleDesc &d = e->sd[si];
@@ -318,6 +320,14 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
             dft_scales.push_back(fs);
             continue;
         }
+        if (!e->fft_two_pass && fs.log2s >= 5 && fs.log2s <= 7) {
+            fs.cta_begin = tile_ctas;
+            fs.ctas_per_frame = (d.tiles + kFftTileTiles(s) - 1) / kFftTileTiles(s);
+            tiles.sc[ntile++] = fs;
+            tile_ctas += fs.ctas_per_frame;
+            tile_smem = std::max(tile_smem, fft_tile_smem_bytes(s));
+            continue;
+        }
         fs.cta_begin = row_ctas;
         fs.ctas_per_frame = static_cast<int>((static_cast<long long>(d.tiles) * (s / 2) + per - 1) / per);
         rows.sc[nfft] = fs;
@@ -330,6 +340,7 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
         smem = std::max(smem, fft_smem_bytes(s));
     }
     rows.S = cols.S = nfft;
+    tiles.S = ntile;
     // Frames go through both passes in groups of up to 256 MB of spectra (15 frames of the
     // 1024^2 x 4-scale shape): fewer, larger launches were measured faster than groups small
     // enough for the row pass's output to stay in L2 (frames/s at 34 / 64 / 100 / 256 MB:
@@ -347,6 +358,14 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
         }
         rows.src = src + f0 * frame_stride;
         rows.first_label = cols.first_label = first_label + f0;
+        if (ntile > 0) {
+            tiles.src = rows.src;
+            tiles.first_label = rows.first_label;
+            fft_tile_kernel<<<dim3(tile_ctas, nf), kFftThreads, tile_smem, e->fft_stream>>>(tiles);
+            CUDA_TRY(cudaGetLastError());
+            e->launches += 1;
+            tr.e->tlaunch[0] += 1;
+        }
         if (nfft > 0) {
             fft_rows_kernel<<<dim3(row_ctas, nf), kFftThreads, smem, e->fft_stream>>>(rows);
             CUDA_TRY(cudaGetLastError());
@@ -688,6 +707,7 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
         return fail(DDM_ERR_INVALID_ARG, "fft_group_frames must be >= 0");
     }
     e->fft_group = cfg->fft_group_frames;
+    e->fft_two_pass = cfg->fft_two_pass ? 1 : 0;
     e->device = cfg->device;
     const bool compat = e->estimator == DDM_EST_COMPAT;
 
@@ -746,6 +766,7 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
             lag_batch_cfg = tv.lag_batch;
             e->lag_geom = tv.lag_geometry;
             e->fft_group = tv.fft_group;
+            e->fft_two_pass = tv.fft_two_pass;
         } else {
             lag_batch_cfg = 0;
         }
@@ -912,6 +933,8 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
 
     // Kernel shared-memory limits (the FFT passes use up to 128 KB)
     if (cudaFuncSetAttribute(fft_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024) != cudaSuccess ||
+        cudaFuncSetAttribute(fft_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(fft_tile_smem_bytes(128))) != cudaSuccess ||
         cudaFuncSetAttribute(fft_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024) != cudaSuccess ||
         cudaFuncSetAttribute(lag_pipe_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
         cudaFuncSetAttribute(lag_pipe_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||
@@ -1343,6 +1366,7 @@ extern "C" int ddm_get_info(const ddm_engine *e, ddm_info *info) {
     info->lag_batch_frames = e->lag_batch;
     info->lag_geometry = e->lag_geom;
     info->fft_group_frames = e->fft_group;
+    info->fft_two_pass = e->fft_two_pass;
     return DDM_OK;
 }
 

@@ -244,16 +244,14 @@ __device__ __forceinline__ float fft_pixel(const uint8_t *p, int pixmode) {
     return static_cast<float>(p[0]);
 }
 
-// Row pass at scale 2^LOG2L: the CTA transforms NT consecutive row pairs of the flattened
-// (tile, pair) index of frame blockIdx.y, rows 2p and 2p+1 packed as real and imaginary parts.
+// Loads NT consecutive row pairs (g0, g0 + 1, ...) of the flattened (tile, pair) index of one
+// frame into the transform slots of fsm, rows 2p and 2p+1 of a tile packed as the real and
+// imaginary parts (zeros past total_pairs).
 template <int LOG2L>
-__device__ __forceinline__ void fft_rows_body(const FftArgs &a, const FftScale &sc, float2 *fsm) {
-    constexpr int L = 1 << LOG2L, TEAM = fft_team(L), NT = fft_per_cta(L), TS = kFftPad(L);
-    constexpr int NX = L / 2 + 1;
+__device__ __forceinline__ void fft_load_pairs(const FftArgs &a, const FftScale &sc, float2 *fsm, int g0,
+                                               int total_pairs, const uint8_t *fsrc) {
+    constexpr int L = 1 << LOG2L, NT = fft_per_cta(L), TS = kFftPad(L);
     constexpr int ITER = NT * L / kFftThreads;
-    const int total_pairs = (1 << (2 * sc.log2side)) * (L / 2);
-    const int g0 = (blockIdx.x - sc.cta_begin) * NT;
-    const uint8_t *fsrc = a.src + blockIdx.y * a.frame_stride;
     if constexpr (L >= 4) {
         if (a.vec4) {  // one byte per pixel, 4-byte aligned rows: 4 pixels of each row per load
 #pragma unroll
@@ -285,7 +283,7 @@ __device__ __forceinline__ void fft_rows_body(const FftArgs &a, const FftScale &
                     d[m] = m == 0 ? v[0] : m == 1 ? v[1] : m == 2 ? v[2] : v[3];
                 }
             }
-            goto loaded;
+            return;
         }
     }
 #pragma unroll
@@ -305,7 +303,17 @@ __device__ __forceinline__ void fft_rows_body(const FftArgs &a, const FftScale &
         }
         fsm[c * TS + fpad(i)] = z;
     }
-loaded:
+}
+
+// Row pass at scale 2^LOG2L: the CTA transforms NT consecutive row pairs of the flattened
+// (tile, pair) index of frame blockIdx.y, rows 2p and 2p+1 packed as real and imaginary parts.
+template <int LOG2L>
+__device__ __forceinline__ void fft_rows_body(const FftArgs &a, const FftScale &sc, float2 *fsm) {
+    constexpr int L = 1 << LOG2L, TEAM = fft_team(L), NT = fft_per_cta(L), TS = kFftPad(L);
+    constexpr int NX = L / 2 + 1;
+    const int total_pairs = (1 << (2 * sc.log2side)) * (L / 2);
+    const int g0 = (blockIdx.x - sc.cta_begin) * NT;
+    fft_load_pairs<LOG2L>(a, sc, fsm, g0, total_pairs, a.src + blockIdx.y * a.frame_stride);
     __syncthreads();
     const int c_me = threadIdx.x & (NT - 1), t = threadIdx.x / NT;  // transforms fastest (no bank conflicts)
     fft_transform<LOG2L>(fsm + c_me * TS, t, a.tw + (L - 2));  // ends with a CTA barrier
@@ -366,6 +374,102 @@ __device__ __forceinline__ void fft_cols_body(const FftArgs &a, const FftScale &
             const int tile = g / NX, col = g - tile * NX;
             base[tile * sc.n + static_cast<long long>(y) * NX + col] = fsm[c * TS + fpad(y)];
         }
+    }
+}
+
+// Both passes of the tiles of side 32, 64 and 128 in one kernel, the tile held in shared
+// memory between them (one HBM write of each half spectrum, no intermediate round trip).
+// A CTA owns kFftTileTiles(L) consecutive tiles of frame blockIdx.y: 1 at 128 (its 64 row pairs
+// in two rounds of 32 transforms), 2 at 64, 8 at 32 (one round). Row rounds load row pairs
+// into the transform slots, transform them and split each into two half-spectrum rows of the
+// tile buffer Yt[tile][y][kx] (rows NXP = NX + 1 float2 apart); column rounds copy NT columns
+// of Yt into the transform slots, transform them along y and store them to the ring slot.
+__host__ __device__ constexpr int kFftTileTiles(int L) {
+    return fft_per_cta(L) / (L / 2) > 1 ? fft_per_cta(L) / (L / 2) : 1;
+}
+__host__ __device__ constexpr int kFftTileNxp(int L) { return L / 2 + 2; }
+inline size_t fft_tile_smem_bytes(int L) {
+    return sizeof(float2) * (static_cast<size_t>(fft_per_cta(L)) * kFftPad(L) +
+                             static_cast<size_t>(kFftTileTiles(L)) * L * kFftTileNxp(L));
+}
+
+template <int LOG2L>
+__device__ __forceinline__ void fft_tile_body(const FftArgs &a, const FftScale &sc, float2 *fsm) {
+    constexpr int L = 1 << LOG2L, TEAM = fft_team(L), NT = fft_per_cta(L), TS = kFftPad(L);
+    constexpr int NX = L / 2 + 1, NXP = kFftTileNxp(L), TPC = kFftTileTiles(L);
+    constexpr int LOG2NT = ilog2c<NT>();
+    constexpr int ITER = NT * L / kFftThreads;
+    float2 *yt = fsm + NT * TS;  // [TPC][L][NXP]
+    const int tiles = 1 << (2 * sc.log2side);
+    const int tile0 = (blockIdx.x - sc.cta_begin) * TPC;
+    const int ntl = tiles - tile0 < TPC ? tiles - tile0 : TPC;  // tiles of this CTA
+    const int pairs = ntl * (L / 2);
+    const int c_me = threadIdx.x & (NT - 1), t = threadIdx.x / NT;
+    const int c_out = threadIdx.x / TEAM, t_out = threadIdx.x & (TEAM - 1);
+    // ---- rows: pairs of the CTA's tiles, NT per round
+    for (int r0 = 0; r0 < pairs; r0 += NT) {
+        fft_load_pairs<LOG2L>(a, sc, fsm, tile0 * (L / 2) + r0, tile0 * (L / 2) + pairs,
+                              a.src + blockIdx.y * a.frame_stride);
+        __syncthreads();
+        fft_transform<LOG2L>(fsm + c_me * TS, t, a.tw + (L - 2));  // ends with a CTA barrier
+        const int g = r0 + c_out;  // pair of the CTA's tiles
+        if (g < pairs) {
+            const float2 *buf = fsm + c_out * TS;
+            const int tl = g >> (LOG2L - 1), py = 2 * (g & (L / 2 - 1));
+            float2 *o = yt + (tl * L + py) * NXP;
+#pragma unroll
+            for (int m = 0; m < (NX + TEAM - 1) / TEAM; m++) {
+                const int k = t_out + m * TEAM;
+                if (k < NX) {
+                    const float2 zk = buf[fpad(k & (L - 1))], zm = buf[fpad((L - k) & (L - 1))];
+                    o[k] = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+                    o[NXP + k] = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+                }
+            }
+        }
+        __syncthreads();  // the slots are reloaded next round; Yt is read by the columns
+    }
+    // ---- columns: (tile, kx) of the CTA's tiles, NT per round
+    const long long slot = (a.first_label + blockIdx.y) % a.R;
+    float2 *base = a.ring + slot * a.E + sc.off;
+    const int cols = ntl * NX;
+    for (int c0 = 0; c0 < cols; c0 += NT) {
+#pragma unroll
+        for (int it = 0; it < ITER; it++) {
+            const int q = threadIdx.x + it * kFftThreads;
+            const int y = q >> LOG2NT, c = q & (NT - 1);
+            const int g = c0 + c;
+            float2 v = make_float2(0.f, 0.f);
+            if (g < cols) {
+                const int tl = g / NX, col = g - tl * NX;
+                v = yt[(tl * L + y) * NXP + col];
+            }
+            fsm[c * TS + fpad(y)] = v;
+        }
+        __syncthreads();
+        fft_transform<LOG2L>(fsm + c_me * TS, t, a.tw + (L - 2));
+#pragma unroll
+        for (int it = 0; it < ITER; it++) {
+            const int q = threadIdx.x + it * kFftThreads;
+            const int y = q >> LOG2NT, c = q & (NT - 1);
+            const int g = c0 + c;
+            if (g < cols) {
+                const int tl = g / NX, col = g - tl * NX;
+                base[(tile0 + tl) * sc.n + static_cast<long long>(y) * NX + col] = fsm[c * TS + fpad(y)];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// grid (sum over the fused scales of tiles / kFftTileTiles, frames); scales of side 32..128
+__global__ void __launch_bounds__(kFftThreads, 2) fft_tile_kernel(FftArgs a) {
+    extern __shared__ float2 fsm[];
+    const FftScale &sc = a.sc[fft_find_scale(a)];
+    switch (sc.log2s) {
+        case 5: fft_tile_body<5>(a, sc, fsm); break;
+        case 6: fft_tile_body<6>(a, sc, fsm); break;
+        default: fft_tile_body<7>(a, sc, fsm); break;
     }
 }
 

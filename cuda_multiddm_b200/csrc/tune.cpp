@@ -6,7 +6,8 @@
 //   lag_geometry      one thread per element (4 consumer warps, 3 CTAs per SM) or two
 //                     (8 consumer warps, 2 CTAs per SM): occupancy against per-entry overhead;
 //   fft_group_frames  frames per FFT launch: fewer, larger launches against keeping the row
-//                     pass's output in L2 and overlapping host copies with the FFT.
+//                     pass's output in L2 and overlapping host copies with the FFT;
+//   fft_two_pass      tiles of side 32..128 in the per-tile kernel or in the two passes.
 // The best values depend on the frame size, scales, tau list and chunk. ddm_autotune times the
 // (J, geometry) candidates, then the FFT groups with the fastest of those, on the caller's
 // shape with synthetic frames resident on the device (the engine's steady state: every timed
@@ -80,14 +81,16 @@ bool tune_lookup(const char *path, const std::string &key, TunedValues *out) {
     while (std::getline(in, line)) {
         const size_t p = line.find(head);
         if (p == std::string::npos) continue;
-        double J = 0, G = 0, F = 0, fps = 0;
+        double J = 0, G = 0, F = 0, V = 0, fps = 0;
         if (!field(p, "lag_batch_frames", &J) || J < 1 || J > 64) return false;
-        field(p, "lag_geometry", &G);  // absent in caches written before the geometry was tuned: 0
+        field(p, "lag_geometry", &G);  // absent in caches written before these were tuned: 0
         field(p, "fft_group_frames", &F);
+        field(p, "fft_two_pass", &V);
         field(p, "frames_per_s", &fps);
         out->lag_batch = static_cast<int>(J);
         out->lag_geometry = (G == 1 && J <= 32) ? 1 : 0;
         out->fft_group = F > 0 ? static_cast<int>(F) : 0;
+        out->fft_two_pass = V == 1 ? 1 : 0;
         out->fps = fps;
         return true;
     }
@@ -123,15 +126,16 @@ bool tune_store(const char *path, const std::string &key, const std::string &ent
     return std::rename(tmp.c_str(), path) == 0;
 }
 
-// Frames/s of one engine with lag_batch_frames = J, lag_geometry = G and fft_group_frames = F
-// on `frames` (device memory): pre-roll until
+// Frames/s of one engine with lag_batch_frames = J, lag_geometry = G, fft_group_frames = F and
+// fft_two_pass = V on `frames` (device memory): pre-roll until
 // every frame has all its lags, then `timed` chunks between two synchronisations.
-int time_candidate(const ddm_config &base, int J, int G, int F, const uint8_t *frames, int n_frames, int timed,
+int time_candidate(const ddm_config &base, int J, int G, int F, int V, const uint8_t *frames, int n_frames, int timed,
                    double *fps) {
     ddm_config c = base;
     c.lag_batch_frames = J;
     c.lag_geometry = G;
     c.fft_group_frames = F;
+    c.fft_two_pass = V;
     c.dump_every = 0;
     ddm_engine *e = nullptr;
     int st = ddm_open(&c, &e);
@@ -200,6 +204,7 @@ extern "C" int ddm_autotune(const ddm_config *cfg, const char *cache_path, ddm_t
         out->lag_batch_frames = tv.lag_batch;
         out->lag_geometry = tv.lag_geometry;
         out->fft_group_frames = tv.fft_group;
+        out->fft_two_pass = tv.fft_two_pass;
         out->frames_per_s = tv.fps;
         out->from_cache = 1;
         return DDM_OK;
@@ -226,42 +231,44 @@ extern "C" int ddm_autotune(const ddm_config *cfg, const char *cache_path, ddm_t
     cands.erase(std::unique(cands.begin(), cands.end()), cands.end());
     const int timed = std::max(4, (8 * 30 + cfg->chunk_frames - 1) / cfg->chunk_frames);
     std::ostringstream tried;
-    int best = 0, best_g = 0, best_f = 0, first_error = DDM_OK;
+    int best = 0, best_g = 0, best_f = 0, best_v = 0, first_error = DDM_OK;
     std::string first_message;
     double best_fps = 0.0;
     // a candidate that cannot run here (e.g. its ring does not fit) is skipped
-    auto run = [&](int J, int G, int F) {
+    auto run = [&](int J, int G, int F, int V) {
         double fps = 0.0;
-        const int st = time_candidate(*cfg, J, G, F, dev, n_frames, timed, &fps);
+        const int st = time_candidate(*cfg, J, G, F, V, dev, n_frames, timed, &fps);
         if (st) {
             if (!first_error) first_error = st, first_message = last_error();
             return;
         }
         char buf[64];
-        std::snprintf(buf, sizeof(buf), "%s\"%d/%d/%d\": %.1f", tried.tellp() > 0 ? ", " : "", J, G, F, fps);
+        std::snprintf(buf, sizeof(buf), "%s\"%d/%d/%d/%d\": %.1f", tried.tellp() > 0 ? ", " : "", J, G, F, V, fps);
         tried << buf;
-        if (fps > best_fps) best_fps = fps, best = J, best_g = G, best_f = F;
+        if (fps > best_fps) best_fps = fps, best = J, best_g = G, best_f = F, best_v = V;
     };
     for (int J : cands)
-        for (int G = 0; G < (J <= 32 ? 2 : 1); G++) run(J, G, 0);
+        for (int G = 0; G < (J <= 32 ? 2 : 1); G++) run(J, G, 0, 0);
     if (best > 0) {
         const int J = best, G = best_g;
         for (int F : kFftGroups)
-            if (F > 0) run(J, G, F);
+            if (F > 0) run(J, G, F, 0);
+        run(J, G, 0, 1);
     }
     cudaFree(dev);
     if (best == 0) return fail(first_error ? first_error : DDM_ERR_CUDA, "ddm_autotune: no candidate ran: " + first_message);
     out->lag_batch_frames = best;
     out->lag_geometry = best_g;
     out->fft_group_frames = best_f;
+    out->fft_two_pass = best_v;
     out->frames_per_s = best_fps;
     out->from_cache = 0;
     if (cache_path && *cache_path) {
         char buf[192];
         std::snprintf(buf, sizeof(buf),
                       "{\"lag_batch_frames\": %d, \"lag_geometry\": %d, \"fft_group_frames\": %d, "
-                      "\"frames_per_s\": %.1f, \"candidates\": {",
-                      best, best_g, best_f, best_fps);
+                      "\"fft_two_pass\": %d, \"frames_per_s\": %.1f, \"candidates\": {",
+                      best, best_g, best_f, best_v, best_fps);
         if (!tune_store(cache_path, key, std::string(buf) + tried.str() + "}}"))
             return fail(DDM_ERR_INVALID_ARG, std::string("ddm_autotune: cannot write the cache ") + cache_path);
     }

@@ -38,6 +38,7 @@ class EngineConfig:
     small_tile_dft: bool = False       # split-BF16 tensor-core DFT for tiles of side 32..128
     lag_geometry: int = 0              # lag kernel: 0 one thread per element, 1 two threads per element
     fft_group_frames: int = 0          # frames per FFT launch (0 = as many as 256 MB of spectra hold)
+    fft_two_pass: bool = False         # True: no per-tile FFT kernel for tiles of side 32..128
     _keep: list = field(default_factory=list, repr=False)
 
     def to_c(self) -> Config:
@@ -52,7 +53,8 @@ class EngineConfig:
                       C.c_float(self.tolerance), self.chunk_frames, est, int(bool(self.multistream)),
                       self.total_frames, self.dump_every, self.hbm_budget_bytes, self.device,
                       C.c_void_p(self.stream) if self.stream else None, self.lag_batch_frames,
-                      int(bool(self.small_tile_dft)), int(self.lag_geometry), int(self.fft_group_frames))
+                      int(bool(self.small_tile_dft)), int(self.lag_geometry), int(self.fft_group_frames),
+                      int(bool(self.fft_two_pass)))
 
 
 def tune_key(cfg: EngineConfig) -> str:
@@ -75,7 +77,8 @@ def autotune(cfg: EngineConfig, cache: str | None = None) -> dict:
     t = Tuning()
     check(lib().ddm_autotune(C.byref(c), cache.encode() if cache else None, C.byref(t)))
     return {"lag_batch_frames": t.lag_batch_frames, "lag_geometry": t.lag_geometry,
-            "fft_group_frames": t.fft_group_frames, "frames_per_s": t.frames_per_s, "from_cache": bool(t.from_cache)}
+            "fft_group_frames": t.fft_group_frames, "fft_two_pass": t.fft_two_pass, "frames_per_s": t.frames_per_s,
+            "from_cache": bool(t.from_cache)}
 
 
 def isf_blocks(isf: np.ndarray, scales: Sequence[int], n_lambda: int, n_tau: int) -> dict:

@@ -97,6 +97,12 @@ typedef struct {
     int fft_group_frames;          /* frames per FFT launch (both passes over every scale);
                                       0 = as many as 256 MB of spectra hold (at least 1). With
                                       lag_batch_frames = -1 the tuned value is used. */
+    int fft_two_pass;              /* 0: tiles of side 32..128 are transformed by one kernel that
+                                      keeps each tile in shared memory between its row and column
+                                      passes; 1: every scale through the two-pass FFT (row pass
+                                      to the ring, column pass in place). Same arithmetic, the
+                                      same spectra bit for bit. With lag_batch_frames = -1 the
+                                      tuned value is used. */
 } ddm_config;
 
 typedef struct ddm_engine ddm_engine;
@@ -155,11 +161,11 @@ int ddm_wait_isf(ddm_engine *e);
  * (unbiased estimator only) with synthetic frames on the device in the engine's steady state,
  * first every lag blocking lag_batch_frames in {16, 24, 30, 32, 64, chunk} with each lag-kernel
  * geometry (lag_geometry 0 and 1; 64 frames run geometry 0 only), then, with the fastest of
- * those, the FFT launch group fft_group_frames in {0 (256 MB of spectra), 4, 8, 16} frames,
- * and returns the fastest combination; with a cache path it first looks the shape up there and
- * afterwards stores the result (a JSON object, one shape key per line, with the frames/s of
- * every candidate as "J/G/F"). Engines opened with lag_batch_frames = -1 take all three tuned
- * values. cfg's small_tile_dft is kept as given (it changes the precision, so it is never
+ * those, the FFT launch group fft_group_frames in {0 (256 MB of spectra), 4, 8, 16} frames and
+ * the two-pass FFT variant (fft_two_pass = 1, 256 MB groups), and returns the fastest
+ * combination; with a cache path it first looks the shape up there and afterwards stores the
+ * result (a JSON object, one shape key per line, with the frames/s of every candidate as
+ * "J/G/F/V"). Engines opened with lag_batch_frames = -1 take all four tuned values. cfg's small_tile_dft is kept as given (it changes the precision, so it is never
  * chosen by timing). ddm_tune_key writes the shape key (frame size and depth, scales, tau
  * count / largest / hash, chunk, estimator, small_tile_dft) into out (capacity bytes, NUL
  * terminated) and returns its length, or -1. */
@@ -169,6 +175,7 @@ typedef struct {
     int from_cache;        /* 1: found in the cache, nothing timed */
     int lag_geometry;      /* the winner's lag-kernel geometry */
     int fft_group_frames;  /* the winner's FFT launch group (0 = the 256 MB rule) */
+    int fft_two_pass;      /* the winner's FFT variant */
 } ddm_tuning;
 int ddm_autotune(const ddm_config *cfg, const char *cache_path, ddm_tuning *out);
 long ddm_tune_key(const ddm_config *cfg, char *out, long capacity);
@@ -254,6 +261,7 @@ typedef struct {
     int lag_batch_frames;          /* frames per lag launch in use (after defaults / tuning) */
     int lag_geometry;              /* lag-kernel geometry in use */
     int fft_group_frames;          /* frames per FFT launch in use */
+    int fft_two_pass;              /* FFT variant in use */
 } ddm_info;
 int ddm_get_info(const ddm_engine *e, ddm_info *info);
 
