@@ -402,7 +402,6 @@ def run_ours(args, w: dict) -> None:
     # Roofline of the lag kernel: its compulsory bytes (counted by the engine per launch) over
     # its CUDA-event time on the engine's stream, against the measured copy bandwidth.
     lag_ms, lag_n, lag_bytes = kstats["lag"]
-    fft_ms, fft_n, fft_bytes = kstats["fft"]
     frames_timed = args.steps * CHUNK
     lag_s = lag_ms / 1000.0
     hbm_peak, peak_kind = measured_peaks()
@@ -432,9 +431,6 @@ def run_ours(args, w: dict) -> None:
                              "frames_per_launch": frames_timed / per_launch,
                              "model_bytes_per_frame": model_bytes_per_frame(w),
                              "model_gbs": model_gbs, "model_frac": model_gbs / hbm_peak},
-                "fft_roofline": {"bound": "hbm", "achieved": fft_bytes / max(fft_ms, 1e-9) / 1e6,
-                                 "frac": fft_bytes / max(fft_ms, 1e-9) / 1e6 / hbm_peak, "unit": "GB/s",
-                                 "bytes": fft_bytes, "ms": fft_ms, "launches": fft_n},
                 "kernels_ms": {k: {"total_ms": v[0], "launches": v[1], "compulsory_bytes": v[2]}
                                for k, v in kstats.items()},
                 "gpu_launches": int(launches), "clocks": clocks}

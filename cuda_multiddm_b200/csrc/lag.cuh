@@ -52,7 +52,7 @@ namespace ddm {
 constexpr int kLagConsumerWarps = 4;
 constexpr int kLagThreads = kLagConsumerWarps * 32 + 32;  // consumers + one producer warp
 constexpr int kLagCtasPerSm = 3;  // registers (128 a thread) and shared memory (~70 KB a CTA) both allow 3
-// Geometries of the kernel (template parameter G): 0 "narrow", the layout above -- one
+// Geometries of the kernel (template parameter GEO): 0 "narrow", the layout above -- one
 // consumer thread per element holding all J <= 32 register frames, four consumer warps, three
 // CTAs per SM; 1 "wide" -- two lanes per element holding J/2 frames each (a warp's partner
 // load then reads 16 elements, one shared-memory wavefront for 32 pairs), eight consumer warps
@@ -201,17 +201,18 @@ struct LagMaps {
 // (n * ngroups * kLagGroup + u) % lag_ring_slots(J). Neither side
 // ever waits for the whole CTA. The CTA handles element blocks block_begin, + block_step, ...
 // below block_end; `maps` may live in kernel parameter space or global memory.
-template <int J, int G = 0>
+template <int J, int GEO = 0>
 __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, float2 *__restrict__ acc, long long E,
                                               const int *__restrict__ table, int *__restrict__ status,
                                               const LagMaps &maps, int block_begin, int block_end, int block_step,
                                               long long wait_cycles) {
-    constexpr int kLanes = lag_lanes(J, G);
+    constexpr int kLanes = lag_lanes(J, GEO);
     constexpr int kJT = J / kLanes;  // register frames per thread
-    constexpr int kElems = lag_cta_elems(J, G);
-    constexpr int kCW = lag_cwarps(G);  // consumer warps; warp kCW produces
-    constexpr int kThreads = lag_threads(G);
-    constexpr uint32_t kSlotBytes = lag_slot_bytes(J, G);
+    constexpr int kElems = lag_cta_elems(J, GEO);
+    constexpr int kCW = lag_cwarps(GEO);  // consumer warps; warp kCW produces
+    constexpr int kThreads = lag_threads(GEO);
+    constexpr uint32_t kSlotBytes = lag_slot_bytes(J, GEO);
+    constexpr int kMap = lag_map_index(J, GEO);  // tensor-map box width of this geometry
     constexpr int kSlots = lag_ring_slots(J);
     constexpr int kGS = lag_group_slots(J);
     constexpr uint32_t kRingBytes = kSlots * kSlotBytes;
@@ -272,7 +273,7 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
                     for (int r = r0; r < r1; r++) {
                         const int run = runs[r];
                         tma_load_2d(smem + (gs * kLagGroup + lag_run_rel(run)) * kSlotBytes,
-                                    &maps.box[lag_map_index(J, G)][lag_run_log2rows(run)], static_cast<int>(e0),
+                                    &maps.box[kMap][lag_run_log2rows(run)], static_cast<int>(e0),
                                     lag_run_slot(run), &full[gs]);
                     }
                 }
@@ -453,12 +454,12 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
 }
 
 // One engine's launch: CTA b handles element blocks b, b + gridDim.x, ... below nblocks.
-template <int J, int G = 0>
-__global__ void __launch_bounds__(lag_threads(G), lag_ctas_per_sm(G))
+template <int J, int GEO = 0>
+__global__ void __launch_bounds__(lag_threads(GEO), lag_ctas_per_sm(GEO))
     lag_pipe_kernel(const float2 *__restrict__ ring, float2 *__restrict__ acc, long long E,
                     const int *__restrict__ table, int *__restrict__ status, const __grid_constant__ LagMaps maps,
                     int nblocks, long long wait_cycles) {
-    lag_pipe_body<J, G>(ring, acc, E, table, status, maps, static_cast<int>(blockIdx.x), nblocks,
+    lag_pipe_body<J, GEO>(ring, acc, E, table, status, maps, static_cast<int>(blockIdx.x), nblocks,
                         static_cast<int>(gridDim.x), wait_cycles);
 }
 
