@@ -152,16 +152,16 @@ def profiled_traffic(w: dict, frames: float):
     p = ROOT / "profiles" / "lag_kernel_c2.txt"
     if not p.exists():
         return None, None
-    src = None
+    src, per_frame = None, None
     for line in p.read_text().splitlines():
         if line.startswith("traffic_source:"):
             src = line.split(":", 1)[1].strip()
         if line.startswith("traffic_bytes_per_frame:"):
             try:
-                return float(line.split(":", 1)[1].split()[0]) * frames, src
+                per_frame = float(line.split(":", 1)[1].split()[0])
             except ValueError:
                 return None, None
-    return None, None
+    return (per_frame * frames, src) if per_frame else (None, None)
 
 
 class ClockSampler:

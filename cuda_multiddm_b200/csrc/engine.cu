@@ -302,9 +302,9 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
     rows.R = e->R;
     rows.tw = e->tw;
     cols = rows;
-    FftArgs tiles = rows;  // scales of side 32..128 through the per-tile kernel
-    int row_ctas = 0, col_ctas = 0, nfft = 0, tile_ctas = 0, ntile = 0;
-    size_t smem = 0, tile_smem = 0;
+    std::vector<FftScale> tile_scales;  // scales of side 32..128 through the per-tile kernel
+    int row_ctas = 0, col_ctas = 0, nfft = 0;
+    size_t smem = 0;
     std::vector<FftScale> dft_scales;  // scales for the tensor-core DFT
     for (int si = 0; si < e->S; si++) {
         const ScaleDesc &d = e->sd[si];
@@ -321,11 +321,9 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
             continue;
         }
         if (!e->fft_two_pass && fs.log2s >= 5 && fs.log2s <= 7) {
-            fs.cta_begin = tile_ctas;
+            fs.cta_begin = 0;
             fs.ctas_per_frame = (d.tiles + kFftTileTiles(s) - 1) / kFftTileTiles(s);
-            tiles.sc[ntile++] = fs;
-            tile_ctas += fs.ctas_per_frame;
-            tile_smem = std::max(tile_smem, fft_tile_smem_bytes(s));
+            tile_scales.push_back(fs);
             continue;
         }
         fs.cta_begin = row_ctas;
@@ -340,7 +338,6 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
         smem = std::max(smem, fft_smem_bytes(s));
     }
     rows.S = cols.S = nfft;
-    tiles.S = ntile;
     // Frames go through both passes in groups of up to 256 MB of spectra (15 frames of the
     // 1024^2 x 4-scale shape): fewer, larger launches were measured faster than groups small
     // enough for the row pass's output to stay in L2 (frames/s at 34 / 64 / 100 / 256 MB:
@@ -358,10 +355,17 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
         }
         rows.src = src + f0 * frame_stride;
         rows.first_label = cols.first_label = first_label + f0;
-        if (ntile > 0) {
-            tiles.src = rows.src;
-            tiles.first_label = rows.first_label;
-            fft_tile_kernel<<<dim3(tile_ctas, nf), kFftThreads, tile_smem, e->fft_stream>>>(tiles);
+        for (const FftScale &fs : tile_scales) {
+            FftArgs t = rows;
+            t.S = 1;
+            t.sc[0] = fs;
+            const dim3 grid(fs.ctas_per_frame, nf);
+            const size_t ts = fft_tile_smem_bytes(fs.s);
+            switch (fs.log2s) {
+                case 5: fft_tile_kernel<5><<<grid, kFftThreads, ts, e->fft_stream>>>(t); break;
+                case 6: fft_tile_kernel<6><<<grid, kFftThreads, ts, e->fft_stream>>>(t); break;
+                default: fft_tile_kernel<7><<<grid, kFftThreads, ts, e->fft_stream>>>(t); break;
+            }
             CUDA_TRY(cudaGetLastError());
             e->launches += 1;
             tr.e->tlaunch[0] += 1;
@@ -933,7 +937,11 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
 
     // Kernel shared-memory limits (the FFT passes use up to 128 KB)
     if (cudaFuncSetAttribute(fft_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024) != cudaSuccess ||
-        cudaFuncSetAttribute(fft_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(fft_tile_kernel<5>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(fft_tile_smem_bytes(32))) != cudaSuccess ||
+        cudaFuncSetAttribute(fft_tile_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(fft_tile_smem_bytes(64))) != cudaSuccess ||
+        cudaFuncSetAttribute(fft_tile_kernel<7>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(fft_tile_smem_bytes(128))) != cudaSuccess ||
         cudaFuncSetAttribute(fft_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024) != cudaSuccess ||
         cudaFuncSetAttribute(lag_pipe_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLagSmemMax) != cudaSuccess ||

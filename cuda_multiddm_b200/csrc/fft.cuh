@@ -462,15 +462,13 @@ __device__ __forceinline__ void fft_tile_body(const FftArgs &a, const FftScale &
     }
 }
 
-// grid (sum over the fused scales of tiles / kFftTileTiles, frames); scales of side 32..128
-__global__ void __launch_bounds__(kFftThreads, 2) fft_tile_kernel(FftArgs a) {
+// One instance per tile side (32, 64, 128), so that each gets the registers its own body
+// needs; grid (tiles / kFftTileTiles(L), frames) of the scale a.sc[0].
+// (side 128 holds 103 KB of shared memory, so two CTAs per SM at most; the others three)
+template <int LOG2L>
+__global__ void __launch_bounds__(kFftThreads, LOG2L == 7 ? 2 : 3) fft_tile_kernel(FftArgs a) {
     extern __shared__ float2 fsm[];
-    const FftScale &sc = a.sc[fft_find_scale(a)];
-    switch (sc.log2s) {
-        case 5: fft_tile_body<5>(a, sc, fsm); break;
-        case 6: fft_tile_body<6>(a, sc, fsm); break;
-        default: fft_tile_body<7>(a, sc, fsm); break;
-    }
+    fft_tile_body<LOG2L>(a, a.sc[0], fsm);
 }
 
 #define DDM_FFT_DISPATCH(BODY)                      \

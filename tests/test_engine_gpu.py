@@ -334,14 +334,19 @@ def test_errors_are_status_codes():
             eng.submit(np.zeros((9, 64, 64), np.uint8))
 
 
-def test_kernel_launches_counted():
+@pytest.mark.parametrize("two_pass", [False, True])
+def test_kernel_launches_counted(two_pass):
     frames = media.synth_video(2, 64, 64, 8, 10)
-    _, _, info = engine_run(frames, [64, 32], [1, 2], [4.0], estimator="unbiased", C=4)
-    # per piece of 4 frames: one row-pass and one column-pass launch over all scales (the
-    # 4 frames fit one L2-resident group); the 8 frames' lag pairs in one launch at finalize
-    # (launches take up to 32 frames); then the two azimuthal stages
-    assert info.kernel_launches == 2 * 2 + 1 + 2
-    assert lib() is not None
+    cfg = EngineConfig(frame_width=64, frame_height=64, scales=[64, 32], taus=[1, 2], lambdas=[4.0], chunk_frames=4,
+                       estimator="unbiased", fft_two_pass=two_pass)
+    with Engine(cfg) as eng:
+        eng.submit(frames)
+        eng.finalize()
+        launches = eng.info().kernel_launches
+    # per piece of 4 frames: one per-tile FFT launch over both scales (sides 32..128), or one
+    # row-pass and one column-pass launch with fft_two_pass; the 8 frames' lag pairs in one
+    # launch at finalize (launches take up to 32 frames); then the two azimuthal stages
+    assert launches == 2 * (2 if two_pass else 1) + 1 + 2
 
 
 def test_wait_timeout_is_reported_and_device_stays_usable():
