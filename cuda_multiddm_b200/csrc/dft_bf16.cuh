@@ -141,7 +141,13 @@ struct DftArgs {
     FftScale sc;
     const uint4 *tables;  // dft_table_bytes(s) bytes, already in the shared-memory layout
     int *status;
+    int vec16;            // 1: one byte per pixel and every tile row 16-byte aligned (16-pixel loads)
 };
+
+// the column step's output of a batch, staged as [tile][ky][kx] over the operand region
+static_assert(128 * (128 / 2 + 1) * 8 <= dft_region_bytes(128) && 2 * 64 * (64 / 2 + 1) * 8 <= dft_region_bytes(64) &&
+                  4 * 32 * (32 / 2 + 1) * 8 <= dft_region_bytes(32),
+              "a batch's half spectra must fit the operand region");
 
 // bounded wait on the CTA's mbarrier; false after kWaitCycles
 __device__ __forceinline__ bool dft_wait(uint64_t *bar, uint32_t parity) { return mbar_wait_bounded(bar, parity); }
@@ -206,19 +212,37 @@ __global__ void __launch_bounds__(kDftThreads, 1) dft_bf16_kernel(DftArgs a) {
             const long long Y = (static_cast<long long>(ty) << LOG2S) + y + a.y_off;
             const long long X0 = (static_cast<long long>(tx) << LOG2S) + a.x_off;
             const uint8_t *row = fsrc + Y * a.row_pitch + X0 * a.bpp;
+            if (a.vec16) {  // bytes: exact in BF16, no lo part; 16 pixels per load
 #pragma unroll 2
-            for (int kg = 0; kg < S / 8; kg++) {
-                __align__(16) __nv_bfloat16 hi[8], lo[8];
+                for (int k16 = 0; k16 < S / 16; k16++) {
+                    uint4 u = make_uint4(0u, 0u, 0u, 0u);
+                    if (valid) u = *reinterpret_cast<const uint4 *>(row + k16 * 16);
+                    const uint32_t w[4] = {u.x, u.y, u.z, u.w};
 #pragma unroll
-                for (int i = 0; i < 8; i++) {
-                    float v = 0.f;
-                    if (valid) v = fft_pixel(row + (kg * 8 + i) * a.bpp, a.pixmode);
-                    hi[i] = __float2bfloat16_rn(v);
-                    lo[i] = __float2bfloat16_rn(v - __bfloat162float(hi[i]));
+                    for (int h = 0; h < 2; h++) {
+                        __align__(16) __nv_bfloat16 hi[8];
+#pragma unroll
+                        for (int i = 0; i < 8; i++)
+                            hi[i] = __float2bfloat16_rn(static_cast<float>((w[h * 2 + i / 4] >> (8 * (i & 3))) & 0xFFu));
+                        *reinterpret_cast<uint4 *>(reg + dft_core_offset(tid, k16 * 16 + h * 8, S)) =
+                            *reinterpret_cast<const uint4 *>(hi);
+                    }
                 }
-                const uint32_t off = dft_core_offset(tid, kg * 8, S);
-                *reinterpret_cast<uint4 *>(reg + off) = *reinterpret_cast<const uint4 *>(hi);
-                if (two_part_a) *reinterpret_cast<uint4 *>(reg + OP128 + off) = *reinterpret_cast<const uint4 *>(lo);
+            } else {
+#pragma unroll 2
+                for (int kg = 0; kg < S / 8; kg++) {
+                    __align__(16) __nv_bfloat16 hi[8], lo[8];
+#pragma unroll
+                    for (int i = 0; i < 8; i++) {
+                        float v = 0.f;
+                        if (valid) v = fft_pixel(row + (kg * 8 + i) * a.bpp, a.pixmode);
+                        hi[i] = __float2bfloat16_rn(v);
+                        lo[i] = __float2bfloat16_rn(v - __bfloat162float(hi[i]));
+                    }
+                    const uint32_t off = dft_core_offset(tid, kg * 8, S);
+                    *reinterpret_cast<uint4 *>(reg + off) = *reinterpret_cast<const uint4 *>(hi);
+                    if (two_part_a) *reinterpret_cast<uint4 *>(reg + OP128 + off) = *reinterpret_cast<const uint4 *>(lo);
+                }
             }
         }
         fence_proxy_async_smem();
@@ -302,28 +326,35 @@ __global__ void __launch_bounds__(kDftThreads, 1) dft_bf16_kernel(DftArgs a) {
         phase++;
         tc_fence_after();
         if (*abort_flag) break;
-        // ---- 5. rows ky < s of Zr, Zi -> the ring slot's half spectra ----------------------
+        // ---- 5. rows ky < s of Zr, Zi -> staged [tile][ky][kx] over the operand region (the
+        // column step has finished reading it), then one coalesced copy of the batch's tiles,
+        // which are consecutive in the ring slot ------------------------------------------------
         {
-            const long long slot = (a.first_label + f) % a.R;
-            float2 *base = a.ring + slot * a.E + sc.off;
+            float2 *stage = reinterpret_cast<float2 *>(reg);
             for (int tl = 0; tl < TPB; tl++) {
-                const int tile = b * TPB + tl;
                 // every warp takes part in the TMEM loads (sync.aligned); lanes ky >= s hold the
-                // padding rows of the tables and write nothing
-                const bool write = tile < tiles && tid < S;
-                float2 *o = base + static_cast<long long>(tile) * sc.n + static_cast<long long>(tid) * NX;
+                // padding rows of the tables and stage nothing
+                float2 *o = stage + (tl * S + tid) * NX;
 #pragma unroll 1
                 for (int k0 = 0; k0 < N1; k0 += 16) {
                     float zr[16], zi[16];
                     tmem_ld16(tmem + lane_base + tl * 2 * N1 + k0, zr);
                     tmem_ld16(tmem + lane_base + tl * 2 * N1 + N1 + k0, zi);
-                    if (write) {
+                    if (tid < S) {
 #pragma unroll
                         for (int i = 0; i < 16; i++)
                             if (k0 + i < NX) o[k0 + i] = make_float2(zr[i], zi[i]);
                     }
                 }
             }
+            __syncthreads();
+            const long long slot = (a.first_label + f) % a.R;
+            const int ntl = tiles - b * TPB < TPB ? tiles - b * TPB : TPB;
+            // sc.n = S * NX is even and every tile starts on a 16-byte boundary of the ring slot
+            uint4 *dst = reinterpret_cast<uint4 *>(a.ring + slot * a.E + sc.off + static_cast<long long>(b * TPB) * sc.n);
+            const uint4 *src = reinterpret_cast<const uint4 *>(stage);
+            const int n16 = ntl * S * NX / 2;
+            for (int i = tid; i < n16; i += kDftThreads) dst[i] = src[i];
         }
         tc_fence_before();
         __syncthreads();

@@ -395,6 +395,10 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
             d.sc = fs;
             d.tables = e->dft_tab[fs.log2s - kDftMinLog2];
             d.status = e->status_d;
+            d.vec16 = (e->bpp == 1 && x_off % 16 == 0 && row_pitch % 16 == 0 && frame_stride % 16 == 0 &&
+                       reinterpret_cast<uintptr_t>(rows.src) % 16 == 0)
+                          ? 1
+                          : 0;
             const long long tiles = 1LL << (2 * fs.log2side), tpb = 128 / fs.s;
             const long long items = (tiles + tpb - 1) / tpb * nf;
             const unsigned grid = static_cast<unsigned>(std::min<long long>(items, e->sms));
