@@ -37,7 +37,7 @@ class Config(C.Structure):
         ("multistream", C.c_int), ("total_frames", C.c_int), ("dump_every", C.c_int),
         ("hbm_budget_bytes", C.c_size_t), ("device", C.c_int), ("stream", C.c_void_p),
         ("lag_batch_frames", C.c_int), ("small_tile_dft", C.c_int), ("lag_geometry", C.c_int),
-        ("fft_group_frames", C.c_int), ("fft_two_pass", C.c_int),
+        ("fft_group_frames", C.c_int), ("fft_per_tile", C.c_int),
     ]
 
 
@@ -45,13 +45,13 @@ class Info(C.Structure):
     _fields_ = [("frames_submitted", C.c_long), ("ring_slots", C.c_int), ("device_bytes", C.c_size_t),
                 ("kernel_launches", C.c_long), ("stream", C.c_void_p), ("frames_needed", C.c_long),
                 ("lag_batch_frames", C.c_int), ("lag_geometry", C.c_int), ("fft_group_frames", C.c_int),
-                ("fft_two_pass", C.c_int)]
+                ("fft_per_tile", C.c_int)]
 
 
 class Tuning(C.Structure):
     _fields_ = [("lag_batch_frames", C.c_int), ("frames_per_s", C.c_double), ("from_cache", C.c_int),
                 ("lag_geometry", C.c_int), ("fft_group_frames", C.c_int),
-                ("fft_two_pass", C.c_int)]
+                ("fft_per_tile", C.c_int)]
 
 
 class ServerConfig(C.Structure):

@@ -354,7 +354,7 @@ int main(int argc, char **argv) {
         cfg.lag_batch_frames = tuned.lag_batch_frames;
         cfg.lag_geometry = tuned.lag_geometry;
         cfg.fft_group_frames = tuned.fft_group_frames;
-        cfg.fft_two_pass = tuned.fft_two_pass;
+        cfg.fft_per_tile = tuned.fft_per_tile;
         if (g_verbose)
             std::fprintf(stderr, "[Info] lag_batch_frames %d, lag_geometry %d, fft_group_frames %d (%s)\n",
                          tuned.lag_batch_frames, tuned.lag_geometry, tuned.fft_group_frames,

@@ -109,7 +109,7 @@ struct ddm_engine {
     bool small_dft = false;
     int lag_geom = 0;  // lag-kernel geometry for launches of up to 32 frames (ddm_config.lag_geometry)
     int fft_group = 0;  // frames per FFT launch (ddm_config.fft_group_frames; 0 = the 256 MB rule)
-    int fft_two_pass = 0;  // 1: no per-tile kernel for tiles of side 32..128 (ddm_config.fft_two_pass)
+    int fft_per_tile = 0;  // 1: tiles of side 32..128 through the per-tile kernel (ddm_config.fft_per_tile)
     uint4 *dft_tab[kDftMaxLog2 - kDftMinLog2 + 1] = {nullptr, nullptr, nullptr};
     uint8_t *stage = nullptr;
     int *tables_d = nullptr, *tables_h = nullptr;
@@ -320,7 +320,7 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
             dft_scales.push_back(fs);
             continue;
         }
-        if (!e->fft_two_pass && fs.log2s >= 5 && fs.log2s <= 7) {
+        if (e->fft_per_tile && fs.log2s >= 5 && fs.log2s <= 7) {
             fs.cta_begin = 0;
             fs.ctas_per_frame = (d.tiles + kFftTileTiles(s) - 1) / kFftTileTiles(s);
             tile_scales.push_back(fs);
@@ -715,7 +715,7 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
         return fail(DDM_ERR_INVALID_ARG, "fft_group_frames must be >= 0");
     }
     e->fft_group = cfg->fft_group_frames;
-    e->fft_two_pass = cfg->fft_two_pass ? 1 : 0;
+    e->fft_per_tile = cfg->fft_per_tile ? 1 : 0;
     e->device = cfg->device;
     const bool compat = e->estimator == DDM_EST_COMPAT;
 
@@ -774,7 +774,7 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
             lag_batch_cfg = tv.lag_batch;
             e->lag_geom = tv.lag_geometry;
             e->fft_group = tv.fft_group;
-            e->fft_two_pass = tv.fft_two_pass;
+            e->fft_per_tile = tv.fft_per_tile;
         } else {
             lag_batch_cfg = 0;
         }
@@ -1378,7 +1378,7 @@ extern "C" int ddm_get_info(const ddm_engine *e, ddm_info *info) {
     info->lag_batch_frames = e->lag_batch;
     info->lag_geometry = e->lag_geom;
     info->fft_group_frames = e->fft_group;
-    info->fft_two_pass = e->fft_two_pass;
+    info->fft_per_tile = e->fft_per_tile;
     return DDM_OK;
 }
 

@@ -59,8 +59,12 @@ __host__ __device__ constexpr int kFftPad(int L) {
 }
 __device__ __forceinline__ int fpad(int i) { return i + (i >> 4); }
 
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Butterfly adds and subtractions as one packed FP32x2 instruction each (sm_100a FADD2 / FFMA2
+// through the compiler's builtins). Both round exactly as the two scalar operations would: a
+// sum is one rounding either way, and b * (-1) + a is exact before its single rounding, i.e.
+// a - b. The spectra are therefore the same bit for bit.
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
 __device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }

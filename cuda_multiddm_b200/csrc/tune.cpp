@@ -7,7 +7,7 @@
 //                     (8 consumer warps, 2 CTAs per SM): occupancy against per-entry overhead;
 //   fft_group_frames  frames per FFT launch: fewer, larger launches against keeping the row
 //                     pass's output in L2 and overlapping host copies with the FFT;
-//   fft_two_pass      tiles of side 32..128 in the per-tile kernel or in the two passes.
+//   fft_per_tile      tiles of side 32..128 in the per-tile kernel or in the two passes.
 // The best values depend on the frame size, scales, tau list and chunk. ddm_autotune times the
 // (J, geometry) candidates, then the FFT groups with the fastest of those, on the caller's
 // shape with synthetic frames resident on the device (the engine's steady state: every timed
@@ -85,12 +85,12 @@ bool tune_lookup(const char *path, const std::string &key, TunedValues *out) {
         if (!field(p, "lag_batch_frames", &J) || J < 1 || J > 64) return false;
         field(p, "lag_geometry", &G);  // absent in caches written before these were tuned: 0
         field(p, "fft_group_frames", &F);
-        field(p, "fft_two_pass", &V);
+        field(p, "fft_per_tile", &V);
         field(p, "frames_per_s", &fps);
         out->lag_batch = static_cast<int>(J);
         out->lag_geometry = (G == 1 && J <= 32) ? 1 : 0;
         out->fft_group = F > 0 ? static_cast<int>(F) : 0;
-        out->fft_two_pass = V == 1 ? 1 : 0;
+        out->fft_per_tile = V == 1 ? 1 : 0;
         out->fps = fps;
         return true;
     }
@@ -127,7 +127,7 @@ bool tune_store(const char *path, const std::string &key, const std::string &ent
 }
 
 // Frames/s of one engine with lag_batch_frames = J, lag_geometry = G, fft_group_frames = F and
-// fft_two_pass = V on `frames` (device memory): pre-roll until
+// fft_per_tile = V on `frames` (device memory): pre-roll until
 // every frame has all its lags, then `timed` chunks between two synchronisations.
 int time_candidate(const ddm_config &base, int J, int G, int F, int V, const uint8_t *frames, int n_frames, int timed,
                    double *fps) {
@@ -135,7 +135,7 @@ int time_candidate(const ddm_config &base, int J, int G, int F, int V, const uin
     c.lag_batch_frames = J;
     c.lag_geometry = G;
     c.fft_group_frames = F;
-    c.fft_two_pass = V;
+    c.fft_per_tile = V;
     c.dump_every = 0;
     ddm_engine *e = nullptr;
     int st = ddm_open(&c, &e);
@@ -204,7 +204,7 @@ extern "C" int ddm_autotune(const ddm_config *cfg, const char *cache_path, ddm_t
         out->lag_batch_frames = tv.lag_batch;
         out->lag_geometry = tv.lag_geometry;
         out->fft_group_frames = tv.fft_group;
-        out->fft_two_pass = tv.fft_two_pass;
+        out->fft_per_tile = tv.fft_per_tile;
         out->frames_per_s = tv.fps;
         out->from_cache = 1;
         return DDM_OK;
@@ -260,14 +260,14 @@ extern "C" int ddm_autotune(const ddm_config *cfg, const char *cache_path, ddm_t
     out->lag_batch_frames = best;
     out->lag_geometry = best_g;
     out->fft_group_frames = best_f;
-    out->fft_two_pass = best_v;
+    out->fft_per_tile = best_v;
     out->frames_per_s = best_fps;
     out->from_cache = 0;
     if (cache_path && *cache_path) {
         char buf[192];
         std::snprintf(buf, sizeof(buf),
                       "{\"lag_batch_frames\": %d, \"lag_geometry\": %d, \"fft_group_frames\": %d, "
-                      "\"fft_two_pass\": %d, \"frames_per_s\": %.1f, \"candidates\": {",
+                      "\"fft_per_tile\": %d, \"frames_per_s\": %.1f, \"candidates\": {",
                       best, best_g, best_f, best_v, best_fps);
         if (!tune_store(cache_path, key, std::string(buf) + tried.str() + "}}"))
             return fail(DDM_ERR_INVALID_ARG, std::string("ddm_autotune: cannot write the cache ") + cache_path);

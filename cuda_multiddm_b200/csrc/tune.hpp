@@ -12,7 +12,7 @@ namespace ddm {
 std::string tune_key(const ddm_config *cfg);
 // The tuned values cached for `key` in the file at `path`, if any.
 struct TunedValues {
-    int lag_batch = 0, lag_geometry = 0, fft_group = 0, fft_two_pass = 0;
+    int lag_batch = 0, lag_geometry = 0, fft_group = 0, fft_per_tile = 0;
     double fps = 0.0;
 };
 bool tune_lookup(const char *path, const std::string &key, TunedValues *out);

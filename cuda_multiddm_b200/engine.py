@@ -38,7 +38,7 @@ class EngineConfig:
     small_tile_dft: bool = False       # split-BF16 tensor-core DFT for tiles of side 32..128
     lag_geometry: int = 0              # lag kernel: 0 one thread per element, 1 two threads per element
     fft_group_frames: int = 0          # frames per FFT launch (0 = as many as 256 MB of spectra hold)
-    fft_two_pass: bool = False         # True: no per-tile FFT kernel for tiles of side 32..128
+    fft_per_tile: bool = False         # True: tiles of side 32..128 through the per-tile FFT kernel
     _keep: list = field(default_factory=list, repr=False)
 
     def to_c(self) -> Config:
@@ -54,7 +54,7 @@ class EngineConfig:
                       self.total_frames, self.dump_every, self.hbm_budget_bytes, self.device,
                       C.c_void_p(self.stream) if self.stream else None, self.lag_batch_frames,
                       int(bool(self.small_tile_dft)), int(self.lag_geometry), int(self.fft_group_frames),
-                      int(bool(self.fft_two_pass)))
+                      int(bool(self.fft_per_tile)))
 
 
 def tune_key(cfg: EngineConfig) -> str:
@@ -77,7 +77,7 @@ def autotune(cfg: EngineConfig, cache: str | None = None) -> dict:
     t = Tuning()
     check(lib().ddm_autotune(C.byref(c), cache.encode() if cache else None, C.byref(t)))
     return {"lag_batch_frames": t.lag_batch_frames, "lag_geometry": t.lag_geometry,
-            "fft_group_frames": t.fft_group_frames, "fft_two_pass": t.fft_two_pass, "frames_per_s": t.frames_per_s,
+            "fft_group_frames": t.fft_group_frames, "fft_per_tile": t.fft_per_tile, "frames_per_s": t.frames_per_s,
             "from_cache": bool(t.from_cache)}
 
 

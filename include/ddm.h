@@ -97,10 +97,11 @@ typedef struct {
     int fft_group_frames;          /* frames per FFT launch (both passes over every scale);
                                       0 = as many as 256 MB of spectra hold (at least 1). With
                                       lag_batch_frames = -1 the tuned value is used. */
-    int fft_two_pass;              /* 0: tiles of side 32..128 are transformed by one kernel that
+    int fft_per_tile;              /* 1: tiles of side 32..128 are transformed by one kernel that
                                       keeps each tile in shared memory between its row and column
-                                      passes; 1: every scale through the two-pass FFT (row pass
-                                      to the ring, column pass in place). Same arithmetic, the
+                                      passes (one HBM write per half spectrum); 0: every scale
+                                      through the two-pass FFT (row pass to the ring, column pass
+                                      in place), measured as fast or faster. Same arithmetic, the
                                       same spectra bit for bit. With lag_batch_frames = -1 the
                                       tuned value is used. */
 } ddm_config;
@@ -162,7 +163,7 @@ int ddm_wait_isf(ddm_engine *e);
  * first every lag blocking lag_batch_frames in {16, 24, 30, 32, 64, chunk} with each lag-kernel
  * geometry (lag_geometry 0 and 1; 64 frames run geometry 0 only), then, with the fastest of
  * those, the FFT launch group fft_group_frames in {0 (256 MB of spectra), 4, 8, 16} frames and
- * the two-pass FFT variant (fft_two_pass = 1, 256 MB groups), and returns the fastest
+ * the per-tile FFT variant (fft_per_tile = 1, 256 MB groups), and returns the fastest
  * combination; with a cache path it first looks the shape up there and afterwards stores the
  * result (a JSON object, one shape key per line, with the frames/s of every candidate as
  * "J/G/F/V"). Engines opened with lag_batch_frames = -1 take all four tuned values. cfg's small_tile_dft is kept as given (it changes the precision, so it is never
@@ -175,7 +176,7 @@ typedef struct {
     int from_cache;        /* 1: found in the cache, nothing timed */
     int lag_geometry;      /* the winner's lag-kernel geometry */
     int fft_group_frames;  /* the winner's FFT launch group (0 = the 256 MB rule) */
-    int fft_two_pass;      /* the winner's FFT variant */
+    int fft_per_tile;      /* the winner's FFT variant */
 } ddm_tuning;
 int ddm_autotune(const ddm_config *cfg, const char *cache_path, ddm_tuning *out);
 long ddm_tune_key(const ddm_config *cfg, char *out, long capacity);
@@ -261,7 +262,7 @@ typedef struct {
     int lag_batch_frames;          /* frames per lag launch in use (after defaults / tuning) */
     int lag_geometry;              /* lag-kernel geometry in use */
     int fft_group_frames;          /* frames per FFT launch in use */
-    int fft_two_pass;              /* FFT variant in use */
+    int fft_per_tile;              /* FFT variant in use */
 } ddm_info;
 int ddm_get_info(const ddm_engine *e, ddm_info *info);
 

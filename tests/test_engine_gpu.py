@@ -334,19 +334,20 @@ def test_errors_are_status_codes():
             eng.submit(np.zeros((9, 64, 64), np.uint8))
 
 
-@pytest.mark.parametrize("two_pass", [False, True])
-def test_kernel_launches_counted(two_pass):
+@pytest.mark.parametrize("per_tile", [False, True])
+def test_kernel_launches_counted(per_tile):
     frames = media.synth_video(2, 64, 64, 8, 10)
     cfg = EngineConfig(frame_width=64, frame_height=64, scales=[64, 32], taus=[1, 2], lambdas=[4.0], chunk_frames=4,
-                       estimator="unbiased", fft_two_pass=two_pass)
+                       estimator="unbiased", fft_per_tile=per_tile)
     with Engine(cfg) as eng:
         eng.submit(frames)
         eng.finalize()
         launches = eng.info().kernel_launches
-    # per piece of 4 frames: one per-tile FFT launch over both scales (sides 32..128), or one
-    # row-pass and one column-pass launch with fft_two_pass; the 8 frames' lag pairs in one
-    # launch at finalize (launches take up to 32 frames); then the two azimuthal stages
-    assert launches == 2 * (2 if two_pass else 1) + 1 + 2
+    # per piece of 4 frames: a row-pass and a column-pass launch over both scales, or with
+    # fft_per_tile one per-tile launch per scale (sides 32..128): two launches either way;
+    # the 8 frames' lag pairs in one launch at finalize (launches take up to 32 frames); then
+    # the two azimuthal stages
+    assert launches == 2 * 2 + 1 + 2
 
 
 def test_wait_timeout_is_reported_and_device_stays_usable():
@@ -398,10 +399,10 @@ def test_wide_lag_geometry_matches_oracle(lag_batch):
 
 @pytest.mark.parametrize("pixel_mode", ["byte0", "u16"])
 def test_per_tile_fft_equals_two_pass(pixel_mode):
-    """Tiles of side 32..128 go through one kernel that keeps each tile in shared memory
-    between its passes (default) or through the two-pass FFT (fft_two_pass): the same
-    arithmetic, so the same spectra bit for bit; an ROI offset and several tiles per CTA
-    included; and within 2e-6 of the FP64 FFT."""
+    """Tiles of side 32..128 go through the two-pass FFT (default) or through one kernel that
+    keeps each tile in shared memory between its passes (fft_per_tile): the same arithmetic,
+    so the same spectra bit for bit; an ROI offset and several tiles per CTA included; and
+    within 2e-6 of the FP64 FFT."""
     M = 256
     if pixel_mode == "u16":
         frames = media.synth_video(44, M + 8, M + 6, 3, 60, amplitude=2000, background=300, noise_sd=-1,
@@ -413,14 +414,14 @@ def test_per_tile_fft_equals_two_pass(pixel_mode):
     raw = np.ascontiguousarray(frames).view(np.uint8).reshape(n, h, w * bpp)
     scales = [256, 128, 64, 32, 16]
     spec = {}
-    for two_pass in (False, True):
+    for per_tile in (False, True):
         cfg = EngineConfig(frame_width=w, frame_height=h, scales=scales, taus=[1], lambdas=[2.0], chunk_frames=4,
                            bytes_per_pixel=bpp, pixel_mode=pixel_mode, x_offset=3, y_offset=5,
-                           fft_two_pass=two_pass)
+                           fft_per_tile=per_tile)
         with Engine(cfg) as eng:
-            assert eng.info().fft_two_pass == int(two_pass)
+            assert eng.info().fft_per_tile == int(per_tile)
             eng.submit(raw)
-            spec[two_pass] = [eng.spectrum(f) for f in range(n)]
+            spec[per_tile] = [eng.spectrum(f) for f in range(n)]
     for f in range(n):
         assert np.array_equal(spec[False][f], spec[True][f])
     pix = O.PIX_U16LE if pixel_mode == "u16" else O.PIX_BYTE0
@@ -430,6 +431,6 @@ def test_per_tile_fft_equals_two_pass(pixel_mode):
         nel = s * (s // 2 + 1)
         for tile in (0, (M // s) ** 2 - 1):
             ref = O.fft2_r2c(tiles[tile])
-            got = spec[False][1][off + tile * nel: off + (tile + 1) * nel].reshape(s, s // 2 + 1)
+            got = spec[True][1][off + tile * nel: off + (tile + 1) * nel].reshape(s, s // 2 + 1)
             assert np.abs(got - ref).max() <= 2e-6 * np.abs(ref).max(), (s, tile)
         off += (M // s) ** 2 * nel

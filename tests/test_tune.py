@@ -18,7 +18,7 @@ CANDIDATES = {16, 24, 30, 32, 64}
 def candidate_keys(chunk: int, best_j: int, best_g: int) -> set:
     """J/G/F/V keys the tuner times: every J with both geometries (64 with the first only) at
     the default FFT group and variant, then the winner's J/G with FFT groups of 4, 8 and 16
-    frames and with the two-pass FFT variant."""
+    frames and with the per-tile FFT variant."""
     js = CANDIDATES | {chunk}
     keys = {f"{j}/{g}/0/0" for j in js for g in ((0, 1) if j <= 32 else (0,))}
     return keys | {f"{best_j}/{best_g}/{f}/0" for f in (4, 8, 16)} | {f"{best_j}/{best_g}/0/1"}
@@ -71,12 +71,12 @@ def test_autotune_times_caches_and_is_used(tmp_path, monkeypatch):
         inf = eng.info()
         assert inf.lag_batch_frames == first["lag_batch_frames"]
         assert inf.lag_geometry == first["lag_geometry"] and inf.fft_group_frames == first["fft_group_frames"]
-        assert inf.fft_two_pass == first["fft_two_pass"]
+        assert inf.fft_per_tile == first["fft_per_tile"]
         eng.submit(frames)
         eng.finalize()
         auto = eng.isf()
     with Engine(cfg(lag_batch_frames=first["lag_batch_frames"], lag_geometry=first["lag_geometry"],
-                    fft_group_frames=first["fft_group_frames"], fft_two_pass=first["fft_two_pass"])) as eng:
+                    fft_group_frames=first["fft_group_frames"], fft_per_tile=first["fft_per_tile"])) as eng:
         eng.submit(frames)
         eng.finalize()
         assert np.array_equal(eng.isf(), auto)
