@@ -16,8 +16,10 @@
 //   -D UM_PER_PX         fit the ISF on the GPU (ddm_fit_isf) and write <out>fit
 //   -E compat|unbiased   estimator (default compat: the reference's own pairing)
 //   -P byte0|u16         16-bit pixel decoding (default byte0: the reference's first byte)
-//   -U CACHE             unbiased estimator: frames per lag launch from the autotuner
-//                        (ddm_autotune; timed once per shape and kept in the JSON file CACHE)
+//   -U CACHE             unbiased estimator: lag blocking, lag-kernel geometry and FFT launch
+//                        shape from the autotuner (ddm_autotune; timed once per shape and kept
+//                        in the JSON file CACHE)
+//   -X                   split-BF16 tensor-core DFT for tiles of side 32..128 (ISF within 1e-3)
 #include <getopt.h>
 #include <unistd.h>
 
@@ -80,8 +82,11 @@ void print_help() {
                  "               coefficient per tile and scale (UMPX: micrometres per pixel)\n"
                  "  -E MODE      compat (default) or unbiased estimator\n"
                  "  -P MODE      byte0 (default) or u16 decoding of 16-bit pixels\n"
-                 "  -U CACHE     with -E unbiased: frames per lag launch picked by the autotuner,\n"
-                 "               timed once per shape and kept in the JSON file CACHE\n");
+                 "  -U CACHE     with -E unbiased: lag blocking, lag-kernel geometry and FFT launch\n"
+                 "               shape picked by the autotuner, timed once per shape and kept in\n"
+                 "               the JSON file CACHE\n"
+                 "  -X           tiles of side 32..128 through the split-BF16 tensor-core DFT\n"
+                 "               (FP32 accumulation; ISF within 1e-3 instead of 1e-5)\n");
 }
 
 // Number text as std::ostream prints a float (6 significant digits), then one space, as
@@ -214,9 +219,10 @@ int main(int argc, char **argv) {
     float tolerance = 1.2f;
     int estimator = DDM_EST_COMPAT, pixel_mode = DDM_PIX_BYTE0;
     std::string tune_cache;  // -U
+    bool small_tile_dft = false;  // -X
 
     for (;;) {
-        int c = getopt(argc, argv, "ho:N:s:x:y:Q:T:S:If:W::vZt:C:MG:F:B:K:AE:P:D:U:");
+        int c = getopt(argc, argv, "ho:N:s:x:y:Q:T:S:If:W::vZt:C:MG:F:B:K:AE:P:D:U:X");
         if (c == -1) break;
         switch (c) {
             case '?':
@@ -256,6 +262,7 @@ int main(int argc, char **argv) {
                 else die("-E takes compat or unbiased");
                 break;
             case 'U': tune_cache = optarg; break;
+            case 'X': small_tile_dft = true; break;
             case 'P':
                 if (!std::strcmp(optarg, "byte0")) pixel_mode = DDM_PIX_BYTE0;
                 else if (!std::strcmp(optarg, "u16")) pixel_mode = DDM_PIX_U16LE;
@@ -347,6 +354,7 @@ int main(int argc, char **argv) {
     cfg.multistream = multistream ? 1 : 0;
     cfg.total_frames = frame_count;
     cfg.dump_every = rolling;
+    cfg.small_tile_dft = small_tile_dft ? 1 : 0;
     if (!tune_cache.empty()) {
         if (estimator != DDM_EST_UNBIASED) die("-U tunes the unbiased estimator (-E unbiased)");
         ddm_tuning tuned;

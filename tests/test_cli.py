@@ -173,3 +173,32 @@ def test_cli_debug_outputs_K_and_A(tmp_path):
                     want = np.abs(O.fft2_r2c(tiles_px[tile]) / (s * s)).reshape(-1) ** 2
                     got = np.array([float(v) for v in rows[f * tiles + tile].split()])
                     assert np.allclose(got, want, rtol=1e-4, atol=1e-6 * want.max())
+
+
+@pytest.mark.gpu
+def test_cli_tensor_core_dft_flag(tmp_path):
+    """-X sends the tiles of side 32..128 through the split-BF16 tensor-core DFT: every ISF
+    file agrees with the FP32 run's within the path's 1e-3 budget (plus half a unit of the
+    6th printed digit), and the larger scale's files, still from the FP32 FFT, are identical."""
+    from cuda_multiddm_b200 import media
+    from cuda_multiddm_b200.media import read_isf_file
+    frames = media.synth_video(19, 256, 256, 40, 120, step_var=1.0)
+    movie = tmp_path / "v.movie"
+    write_movie(movie, frames)
+    ps, pt, pl = write_params(tmp_path, (256, 128, 64), (1, 2, 3, 5, 8), (4.0, 8.0, 16.0, 32.0))
+    base = ["-N", "40", "-C", "10", "-Q", str(pl), "-T", str(pt), "-S", str(ps), "-M", "-f", str(movie),
+            "-E", "unbiased"]
+    for tag, extra in (("a_", []), ("b_", ["-X"])):
+        r = run_cli(["-o", str(tmp_path / tag), *base, *extra])
+        assert r.returncode == 0, r.stderr
+    n = 0
+    for fa in sorted(tmp_path.glob("a_*")):
+        fb = tmp_path / fa.name.replace("a_", "b_", 1)
+        _, _, ia = read_isf_file(fa)
+        _, _, ib = read_isf_file(fb)
+        if fa.name.startswith("a_256"):
+            assert fa.read_text() == fb.read_text()
+        tol = 1e-3 * np.abs(ia) + sig_digit_tolerance(ia) + sig_digit_tolerance(ib)
+        assert np.all(np.abs(ia - ib) <= tol), fa.name
+        n += 1
+    assert n == 1 + 4 + 16
