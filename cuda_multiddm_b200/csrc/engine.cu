@@ -303,7 +303,7 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
     rows.tw = e->tw;
     cols = rows;
     std::vector<FftScale> tile_scales;  // scales of side 32..128 through the per-tile kernel
-    int nfft = 0;
+    int row_ctas = 0, col_ctas = 0, nfft = 0;
     size_t smem = 0;
     std::vector<FftScale> dft_scales;  // scales for the tensor-core DFT
     for (int si = 0; si < e->S; si++) {
@@ -326,11 +326,14 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
             tile_scales.push_back(fs);
             continue;
         }
-        fs.cta_begin = 0;  // set per group of frames (scale-major grids)
+        fs.cta_begin = row_ctas;
         fs.ctas_per_frame = static_cast<int>((static_cast<long long>(d.tiles) * (s / 2) + per - 1) / per);
         rows.sc[nfft] = fs;
+        row_ctas += fs.ctas_per_frame;
+        fs.cta_begin = col_ctas;
         fs.ctas_per_frame = static_cast<int>((static_cast<long long>(d.tiles) * (s / 2 + 1) + per - 1) / per);
         cols.sc[nfft] = fs;
+        col_ctas += fs.ctas_per_frame;
         nfft++;
         smem = std::max(smem, fft_smem_bytes(s));
     }
@@ -368,17 +371,9 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
             tr.e->tlaunch[0] += 1;
         }
         if (nfft > 0) {
-            // scale-major 1-D grids: scale i's CTAs of all nf frames start at cta_begin
-            int rb = 0, cb = 0;
-            for (int i = 0; i < nfft; i++) {
-                rows.sc[i].cta_begin = rb;
-                cols.sc[i].cta_begin = cb;
-                rb += rows.sc[i].ctas_per_frame * nf;
-                cb += cols.sc[i].ctas_per_frame * nf;
-            }
-            fft_rows_kernel<<<rb, kFftThreads, smem, e->fft_stream>>>(rows);
+            fft_rows_kernel<<<dim3(row_ctas, nf), kFftThreads, smem, e->fft_stream>>>(rows);
             CUDA_TRY(cudaGetLastError());
-            fft_cols_kernel<<<cb, kFftThreads, smem, e->fft_stream>>>(cols);
+            fft_cols_kernel<<<dim3(col_ctas, nf), kFftThreads, smem, e->fft_stream>>>(cols);
             CUDA_TRY(cudaGetLastError());
             e->launches += 2;
             tr.e->tlaunch[0] += 2;

@@ -217,10 +217,7 @@ __device__ __forceinline__ void fft_transform(float2 *buf, int t, const float2 *
 struct FftScale {
     int s, log2s, tiles_side, log2side;
     int ctas_per_frame;
-    int cta_begin;        // first CTA (blockIdx.x) of this scale: the row and column passes order
-                          // their grid scale-major (all of a scale's CTAs over the group's frames,
-                          // then the next scale), so the CTAs resident at a time mostly run one
-                          // scale's code; the per-tile kernel has one scale per launch
+    int cta_begin;        // first CTA (blockIdx.x) of this scale
     long long n, off;     // elements per tile, offset of the scale in a frame
 };
 
@@ -244,15 +241,6 @@ __device__ __forceinline__ int fft_find_scale(const FftArgs &a) {
     int si = 0;
     while (si + 1 < a.S && static_cast<int>(blockIdx.x) >= a.sc[si + 1].cta_begin) si++;
     return si;
-}
-
-// (CTA within the frame, frame of the group) of this block in the scale-major order
-struct FftPos {
-    int cta, frame;
-};
-__device__ __forceinline__ FftPos fft_locate(const FftScale &sc) {
-    const int rel = static_cast<int>(blockIdx.x) - sc.cta_begin;
-    return FftPos{rel % sc.ctas_per_frame, rel / sc.ctas_per_frame};
 }
 
 __device__ __forceinline__ float fft_pixel(const uint8_t *p, int pixmode) {
@@ -322,14 +310,14 @@ __device__ __forceinline__ void fft_load_pairs(const FftArgs &a, const FftScale 
 }
 
 // Row pass at scale 2^LOG2L: the CTA transforms NT consecutive row pairs of the flattened
-// (tile, pair) index of frame pos.frame, rows 2p and 2p+1 packed as real and imaginary parts.
+// (tile, pair) index of frame blockIdx.y, rows 2p and 2p+1 packed as real and imaginary parts.
 template <int LOG2L>
-__device__ __forceinline__ void fft_rows_body(const FftArgs &a, const FftScale &sc, float2 *fsm, FftPos pos) {
+__device__ __forceinline__ void fft_rows_body(const FftArgs &a, const FftScale &sc, float2 *fsm) {
     constexpr int L = 1 << LOG2L, TEAM = fft_team(L), NT = fft_per_cta(L), TS = kFftPad(L);
     constexpr int NX = L / 2 + 1;
     const int total_pairs = (1 << (2 * sc.log2side)) * (L / 2);
-    const int g0 = pos.cta * NT;
-    fft_load_pairs<LOG2L>(a, sc, fsm, g0, total_pairs, a.src + static_cast<long long>(pos.frame) * a.frame_stride);
+    const int g0 = (blockIdx.x - sc.cta_begin) * NT;
+    fft_load_pairs<LOG2L>(a, sc, fsm, g0, total_pairs, a.src + blockIdx.y * a.frame_stride);
     __syncthreads();
     const int c_me = threadIdx.x & (NT - 1), t = threadIdx.x / NT;  // transforms fastest (no bank conflicts)
     fft_transform<LOG2L>(fsm + c_me * TS, t, a.tw + (L - 2));  // ends with a CTA barrier
@@ -341,7 +329,7 @@ __device__ __forceinline__ void fft_rows_body(const FftArgs &a, const FftScale &
     if (g >= total_pairs) return;
     const int tile = g >> (LOG2L - 1 > 0 ? LOG2L - 1 : 0);
     const int py = 2 * (g & (L / 2 - 1));
-    const long long slot = (a.first_label + pos.frame) % a.R;
+    const long long slot = (a.first_label + blockIdx.y) % a.R;
     float2 *o = a.ring + slot * a.E + sc.off + tile * sc.n + static_cast<long long>(py) * NX;
 #pragma unroll
     for (int m = 0; m < (NX + TEAM - 1) / TEAM; m++) {
@@ -355,16 +343,16 @@ __device__ __forceinline__ void fft_rows_body(const FftArgs &a, const FftScale &
 }
 
 // Column pass at scale 2^LOG2L: NT consecutive columns of the flattened (tile, kx) index of
-// frame pos.frame, transformed along y in place.
+// frame blockIdx.y, transformed along y in place.
 template <int LOG2L>
-__device__ __forceinline__ void fft_cols_body(const FftArgs &a, const FftScale &sc, float2 *fsm, FftPos pos) {
+__device__ __forceinline__ void fft_cols_body(const FftArgs &a, const FftScale &sc, float2 *fsm) {
     constexpr int L = 1 << LOG2L, TEAM = fft_team(L), NT = fft_per_cta(L), TS = kFftPad(L);
     constexpr int NX = L / 2 + 1;
     constexpr int LOG2NT = ilog2c<NT>();
     constexpr int ITER = NT * L / kFftThreads;
     const int total_cols = (1 << (2 * sc.log2side)) * NX;
-    const int g0 = pos.cta * NT;
-    const long long slot = (a.first_label + pos.frame) % a.R;
+    const int g0 = (blockIdx.x - sc.cta_begin) * NT;
+    const long long slot = (a.first_label + blockIdx.y) % a.R;
     float2 *base = a.ring + slot * a.E + sc.off;
 #pragma unroll
     for (int it = 0; it < ITER; it++) {
@@ -487,34 +475,32 @@ __global__ void __launch_bounds__(kFftThreads, LOG2L == 7 ? 2 : 3) fft_tile_kern
     fft_tile_body<LOG2L>(a, a.sc[0], fsm);
 }
 
-#define DDM_FFT_DISPATCH(BODY)                           \
-    switch (sc.log2s) {                                  \
-        case 1: BODY<1>(a, sc, fsm, pos); break;         \
-        case 2: BODY<2>(a, sc, fsm, pos); break;         \
-        case 3: BODY<3>(a, sc, fsm, pos); break;         \
-        case 4: BODY<4>(a, sc, fsm, pos); break;         \
-        case 5: BODY<5>(a, sc, fsm, pos); break;         \
-        case 6: BODY<6>(a, sc, fsm, pos); break;         \
-        case 7: BODY<7>(a, sc, fsm, pos); break;         \
-        case 8: BODY<8>(a, sc, fsm, pos); break;         \
-        case 9: BODY<9>(a, sc, fsm, pos); break;         \
-        case 10: BODY<10>(a, sc, fsm, pos); break;       \
-        case 11: BODY<11>(a, sc, fsm, pos); break;       \
-        default: BODY<12>(a, sc, fsm, pos); break;       \
+#define DDM_FFT_DISPATCH(BODY)                      \
+    switch (sc.log2s) {                             \
+        case 1: BODY<1>(a, sc, fsm); break;         \
+        case 2: BODY<2>(a, sc, fsm); break;         \
+        case 3: BODY<3>(a, sc, fsm); break;         \
+        case 4: BODY<4>(a, sc, fsm); break;         \
+        case 5: BODY<5>(a, sc, fsm); break;         \
+        case 6: BODY<6>(a, sc, fsm); break;         \
+        case 7: BODY<7>(a, sc, fsm); break;         \
+        case 8: BODY<8>(a, sc, fsm); break;         \
+        case 9: BODY<9>(a, sc, fsm); break;         \
+        case 10: BODY<10>(a, sc, fsm); break;       \
+        case 11: BODY<11>(a, sc, fsm); break;       \
+        default: BODY<12>(a, sc, fsm); break;       \
     }
 
-// 1-D grid of sum over scales of ctas_per_frame x frames, scale-major (FftScale::cta_begin)
+// grid (sum of ctas_per_frame, frames)
 __global__ void __launch_bounds__(kFftThreads, 4) fft_rows_kernel(FftArgs a) {
     extern __shared__ float2 fsm[];
     const FftScale &sc = a.sc[fft_find_scale(a)];
-    const FftPos pos = fft_locate(sc);
     DDM_FFT_DISPATCH(fft_rows_body)
 }
 
 __global__ void __launch_bounds__(kFftThreads, 4) fft_cols_kernel(FftArgs a) {
     extern __shared__ float2 fsm[];
     const FftScale &sc = a.sc[fft_find_scale(a)];
-    const FftPos pos = fft_locate(sc);
     DDM_FFT_DISPATCH(fft_cols_body)
 }
 #undef DDM_FFT_DISPATCH
