@@ -192,6 +192,75 @@ __device__ __forceinline__ void stockham_pass(float2 *buf, int t, const float2 *
     __syncthreads();
 }
 
+// The same pass with its inputs read by load(i) and its outputs written by store(i, v) (element
+// i of the transform) instead of the shared-memory buffer, and no barriers: for a first pass
+// that reads global memory or a last pass that writes it, the caller orders the rest.
+template <int LOG2L, int R, int NS, class Load, class Store>
+__device__ __forceinline__ void stockham_pass_io(int t, const float2 *__restrict__ tw, Load load, Store store) {
+    constexpr int L = 1 << LOG2L;
+    constexpr int TEAM = L >= 16 ? L / 16 : 1;
+    constexpr int STRIDE = L / R;
+    constexpr int G = STRIDE / TEAM < 1 ? 1 : STRIDE / TEAM;
+    constexpr int SHIFT = LOG2L - ilog2c<NS>() - ilog2c<R>();
+    float2 v[G * R];
+#pragma unroll
+    for (int g = 0; g < G; g++) {
+        const int j = t + g * TEAM;
+        const int jm = j & (NS - 1);
+        float2 wp[R];
+        if constexpr (NS > 1) {
+#pragma unroll
+            for (int b = 1; b < R; b <<= 1) wp[b] = __ldg(tw + ((jm * b) << SHIFT));
+#pragma unroll
+            for (int r = 3; r < R; r++)
+                if (r & (r - 1)) wp[r] = cmulf(wp[r & (r - 1)], wp[r & -r]);
+        }
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            float2 x = load(j + r * STRIDE);
+            if (NS > 1 && r > 0) x = cmulf(x, wp[r]);
+            v[g * R + r] = x;
+        }
+    }
+#pragma unroll
+    for (int g = 0; g < G; g++) {
+        dft_reg<R>(v + g * R);
+        const int j = t + g * TEAM;
+        const int idx = (j & ~(NS - 1)) * R + (j & (NS - 1));
+#pragma unroll
+        for (int r = 0; r < R; r++) store(idx + r * NS, v[g * R + r]);
+    }
+}
+
+// Forward transform of length 2^LOG2L whose input is read by load(i) and whose output is
+// written by store(i, v) in global memory: the first pass loads its inputs into registers
+// straight from global memory and the last pass stores straight to it; the passes between
+// run in place in the shared-memory buffer as fft_transform's do. The same passes and
+// arithmetic as fft_transform (same results bit for bit), with one shared-memory round trip
+// of the transform's data fewer at each end.
+template <int LOG2L, int NS = 1, class Load, class Store>
+__device__ __forceinline__ void fft_transform_io(float2 *buf, int t, const float2 *__restrict__ tw, Load load,
+                                                 Store store) {
+    constexpr int L = 1 << LOG2L;
+    constexpr int left = LOG2L - ilog2c<NS>();
+    constexpr int R = L < 16 ? L : (left >= 4 ? 16 : (1 << left));
+    constexpr bool first = NS == 1, last = NS * R == L;
+    auto sload = [buf](int i) { return buf[fpad(i)]; };
+    auto sstore = [buf](int i, float2 v) { buf[fpad(i)] = v; };
+    if constexpr (first && last) {  // one pass (team of one thread): global to global
+        stockham_pass_io<LOG2L, R, NS>(t, tw, load, store);
+    } else if constexpr (first) {
+        stockham_pass_io<LOG2L, R, NS>(t, tw, load, sstore);
+        __syncthreads();
+        fft_transform_io<LOG2L, NS * R>(buf, t, tw, load, store);
+    } else if constexpr (last) {  // after a barrier: the previous pass's stores are visible
+        stockham_pass_io<LOG2L, R, NS>(t, tw, sload, store);
+    } else {
+        stockham_pass<LOG2L, R, NS>(buf, t, tw);  // in place, ends with a barrier
+        fft_transform_io<LOG2L, NS * R>(buf, t, tw, load, store);
+    }
+}
+
 // Forward transform of length 2^LOG2L: radix-16 passes, then one pass of radix 2, 4 or 8.
 template <int LOG2L, int NS = 1>
 __device__ __forceinline__ void fft_transform(float2 *buf, int t, const float2 *__restrict__ tw) {
@@ -346,39 +415,25 @@ __device__ __forceinline__ void fft_rows_body(const FftArgs &a, const FftScale &
 // frame blockIdx.y, transformed along y in place.
 template <int LOG2L>
 __device__ __forceinline__ void fft_cols_body(const FftArgs &a, const FftScale &sc, float2 *fsm) {
-    constexpr int L = 1 << LOG2L, TEAM = fft_team(L), NT = fft_per_cta(L), TS = kFftPad(L);
+    constexpr int L = 1 << LOG2L, NT = fft_per_cta(L), TS = kFftPad(L);
     constexpr int NX = L / 2 + 1;
-    constexpr int LOG2NT = ilog2c<NT>();
-    constexpr int ITER = NT * L / kFftThreads;
     const int total_cols = (1 << (2 * sc.log2side)) * NX;
     const int g0 = (blockIdx.x - sc.cta_begin) * NT;
     const long long slot = (a.first_label + blockIdx.y) % a.R;
     float2 *base = a.ring + slot * a.E + sc.off;
-#pragma unroll
-    for (int it = 0; it < ITER; it++) {
-        const int q = threadIdx.x + it * kFftThreads;
-        const int y = q >> LOG2NT, c = q & (NT - 1);
-        const int g = g0 + c;
-        float2 v = make_float2(0.f, 0.f);
-        if (g < total_cols) {
-            const int tile = g / NX, col = g - tile * NX;
-            v = base[tile * sc.n + static_cast<long long>(y) * NX + col];
-        }
-        fsm[c * TS + fpad(y)] = v;
-    }
-    __syncthreads();
-    const int c_me = threadIdx.x & (NT - 1), t = threadIdx.x / NT;  // transforms fastest (no bank conflicts)
-    fft_transform<LOG2L>(fsm + c_me * TS, t, a.tw + (L - 2));
-#pragma unroll
-    for (int it = 0; it < ITER; it++) {
-        const int q = threadIdx.x + it * kFftThreads;
-        const int y = q >> LOG2NT, c = q & (NT - 1);
-        const int g = g0 + c;
-        if (g < total_cols) {
-            const int tile = g / NX, col = g - tile * NX;
-            base[tile * sc.n + static_cast<long long>(y) * NX + col] = fsm[c * TS + fpad(y)];
-        }
-    }
+    // transforms fastest (no bank conflicts in the shared-memory passes); a half-warp's global
+    // accesses cover NT consecutive columns (of one row of a tile) times 16/NT rows
+    const int c_me = threadIdx.x & (NT - 1), t = threadIdx.x / NT;
+    const int g = g0 + c_me;
+    const bool valid = g < total_cols;  // threads past the last column still take every barrier
+    const int tile = valid ? g / NX : 0, col = valid ? g - tile * NX : 0;
+    float2 *colp = base + tile * sc.n + col;
+    fft_transform_io<LOG2L>(
+        fsm + c_me * TS, t, a.tw + (L - 2),
+        [&](int y) { return valid ? colp[static_cast<long long>(y) * NX] : make_float2(0.f, 0.f); },
+        [&](int y, float2 v) {
+            if (valid) colp[static_cast<long long>(y) * NX] = v;
+        });
 }
 
 // Both passes of the tiles of side 32, 64 and 128 in one kernel, the tile held in shared
