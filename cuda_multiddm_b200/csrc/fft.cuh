@@ -441,8 +441,8 @@ __device__ __forceinline__ void fft_cols_body(const FftArgs &a, const FftScale &
 // A CTA owns kFftTileTiles(L) consecutive tiles of frame blockIdx.y: 1 at 128 (its 64 row pairs
 // in two rounds of 32 transforms), 2 at 64, 8 at 32 (one round). Row rounds load row pairs
 // into the transform slots, transform them and split each into two half-spectrum rows of the
-// tile buffer Yt[tile][y][kx] (rows NXP = NX + 1 float2 apart); column rounds copy NT columns
-// of Yt into the transform slots, transform them along y and store them to the ring slot.
+// tile buffer Yt[tile][y][kx] (rows NXP float2 apart); column rounds transform NT columns of Yt
+// along y, the first pass reading Yt and the last writing the ring slot directly.
 __host__ __device__ constexpr int kFftTileTiles(int L) {
     return fft_per_cta(L) / (L / 2) > 1 ? fft_per_cta(L) / (L / 2) : 1;
 }
@@ -456,8 +456,6 @@ template <int LOG2L>
 __device__ __forceinline__ void fft_tile_body(const FftArgs &a, const FftScale &sc, float2 *fsm) {
     constexpr int L = 1 << LOG2L, TEAM = fft_team(L), NT = fft_per_cta(L), TS = kFftPad(L);
     constexpr int NX = L / 2 + 1, NXP = kFftTileNxp(L), TPC = kFftTileTiles(L);
-    constexpr int LOG2NT = ilog2c<NT>();
-    constexpr int ITER = NT * L / kFftThreads;
     float2 *yt = fsm + NT * TS;  // [TPC][L][NXP]
     const int tiles = 1 << (2 * sc.log2side);
     const int tile0 = (blockIdx.x - sc.cta_begin) * TPC;
@@ -493,31 +491,20 @@ __device__ __forceinline__ void fft_tile_body(const FftArgs &a, const FftScale &
     float2 *base = a.ring + slot * a.E + sc.off;
     const int cols = ntl * NX;
     for (int c0 = 0; c0 < cols; c0 += NT) {
-#pragma unroll
-        for (int it = 0; it < ITER; it++) {
-            const int q = threadIdx.x + it * kFftThreads;
-            const int y = q >> LOG2NT, c = q & (NT - 1);
-            const int g = c0 + c;
-            float2 v = make_float2(0.f, 0.f);
-            if (g < cols) {
-                const int tl = g / NX, col = g - tl * NX;
-                v = yt[(tl * L + y) * NXP + col];
-            }
-            fsm[c * TS + fpad(y)] = v;
-        }
-        __syncthreads();
-        fft_transform<LOG2L>(fsm + c_me * TS, t, a.tw + (L - 2));
-#pragma unroll
-        for (int it = 0; it < ITER; it++) {
-            const int q = threadIdx.x + it * kFftThreads;
-            const int y = q >> LOG2NT, c = q & (NT - 1);
-            const int g = c0 + c;
-            if (g < cols) {
-                const int tl = g / NX, col = g - tl * NX;
-                base[(tile0 + tl) * sc.n + static_cast<long long>(y) * NX + col] = fsm[c * TS + fpad(y)];
-            }
-        }
-        __syncthreads();
+        // the first pass reads its column of Yt straight into registers, the last writes the
+        // half spectrum's column straight to the ring slot (fft_transform_io)
+        const int g = c0 + c_me;
+        const bool valid = g < cols;  // threads past the last column still take every barrier
+        const int tl = valid ? g / NX : 0, col = valid ? g - tl * NX : 0;
+        const float2 *ycol = yt + tl * L * NXP + col;
+        float2 *ocol = base + (tile0 + tl) * sc.n + col;
+        fft_transform_io<LOG2L>(
+            fsm + c_me * TS, t, a.tw + (L - 2),
+            [&](int y) { return valid ? ycol[y * NXP] : make_float2(0.f, 0.f); },
+            [&](int y, float2 v) {
+                if (valid) ocol[static_cast<long long>(y) * NX] = v;
+            });
+        __syncthreads();  // the next round's first pass rewrites the transform slots
     }
 }
 
