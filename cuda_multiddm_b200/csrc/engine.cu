@@ -19,6 +19,7 @@
 #include <cstring>
 #include <limits>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/ddm.h"
@@ -79,6 +80,9 @@ struct ddm_engine {
     int C = 30, estimator = DDM_EST_UNBIASED, multistream = 1, N = 0, G = 0, device = 0;
     int M = 0, S = 0, T = 0, Q = 0, tau_max = 0;
     int sms = 0;  // SMs of the device (persistent lag grid)
+    // resident CTAs per SM of a lag kernel instance (key J * kLagGeoms + G) at a launch's
+    // dynamic shared-memory size: the persistent grid is that many CTAs per SM
+    std::vector<std::tuple<int, size_t, int>> lag_resident;
     long long E = 0;
     std::vector<ScaleDesc> sd;
     long long isf_size = 0;
@@ -423,6 +427,19 @@ int launch_fft(ddm_engine *e, const uint8_t *src, long long frame_stride, long l
 // Lag launches
 // ---------------------------------------------------------------------------------
 
+// CTAs of `kernel` that fit on one SM with `smem` bytes of dynamic shared memory each (the
+// register and shared-memory budgets of the instance), cached per engine.
+template <class K>
+int lag_resident_ctas(ddm_engine *e, int key, size_t smem, K kernel, int threads) {
+    for (const auto &r : e->lag_resident)
+        if (std::get<0>(r) == key && std::get<1>(r) == smem) return std::get<2>(r);
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem) != cudaSuccess || n < 1) n = 1;
+    if (e->lag_resident.size() > 64) e->lag_resident.clear();
+    e->lag_resident.emplace_back(key, smem, n);
+    return n;
+}
+
 int launch_lag(ddm_engine *e, const Launch &L) {
     if (L.nreg <= 0 || L.ent_acc.empty()) return DDM_OK;
     const int J = lag_pick_j(L.nreg);
@@ -470,15 +487,20 @@ int launch_lag(ddm_engine *e, const Launch &L) {
     }
     TimedRange tr(e, 1);
     // persistent grid: every resident CTA walks element blocks blockIdx.x, + gridDim.x, ...
-    const unsigned grid = std::min<unsigned>(blocks, static_cast<unsigned>(lag_ctas_per_sm(G) * e->sms));
+    // (as many CTAs as fit on the SMs at once: lag_ctas_per_sm(G) per SM unless a large pair
+    // table leaves room for fewer)
     switch (J * kLagGeoms + G) {
 #define LAG_CASE(JJ, GG)                                                                                     \
-    case JJ * kLagGeoms + GG:                                                                                \
+    case JJ * kLagGeoms + GG: {                                                                              \
+        const int per_sm = lag_resident_ctas(e, JJ * kLagGeoms + GG, smem, lag_pipe_kernel<JJ, GG>,         \
+                                             lag_threads(GG));                                               \
+        const unsigned grid = std::min<unsigned>(blocks, static_cast<unsigned>(per_sm * e->sms));          \
         lag_pipe_kernel<JJ, GG><<<grid, lag_threads(GG), smem, e->stream>>>(e->ring, e->acc, e->E, td,      \
                                                                            e->status_d, e->maps,             \
                                                                            static_cast<int>(blocks),         \
                                                                            e->wait_cycles);                  \
-        break;
+        break;                                                                                               \
+    }
         LAG_CASE(4, 0) LAG_CASE(8, 0) LAG_CASE(16, 0) LAG_CASE(20, 0) LAG_CASE(24, 0) LAG_CASE(30, 0)
         LAG_CASE(32, 0) LAG_CASE(64, 0)
         LAG_CASE(4, 1) LAG_CASE(8, 1) LAG_CASE(16, 1) LAG_CASE(20, 1) LAG_CASE(24, 1) LAG_CASE(30, 1)

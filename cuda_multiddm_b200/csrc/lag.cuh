@@ -18,8 +18,11 @@
 // refills a group once every consumer warp has arrived on its "empty" mbarrier. Consumers
 // wait once per window for every group it reaches, then release the groups no later window
 // reads. The |dF|^2 arithmetic is a packed FP32x2 add (FADD2) and two scalar FMAs per pair.
-// Accumulators (FP32 sum + Kahan compensation, 8 B) are loaded three entries ahead with
-// plain coalesced loads and written back once per entry.
+// Accumulators (FP32 sum + Kahan compensation, 8 B) are prefetched kLagAccSlots entries ahead
+// by each consumer thread with cp.async into a private shared-memory ring and written back
+// once per entry with plain coalesced stores. (Prefetching into registers instead did not
+// work: the loop rotates the prefetched values from register to register every entry, and
+// each such move waits for its load, so the loads were exposed one entry after their issue.)
 //
 // Fused runs. With the register frames in registers and the partners in shared memory, the
 // kernel is bound by its shared-memory loads (one 8-byte load per pair) as much as by HBM:
@@ -78,6 +81,11 @@ constexpr int kLagRunKinds = 4;  // box heights 1, 2, 4, 8
 // register frame q - r). Table flag bits per entry: 1 = full window, 2 = first of a run.
 constexpr int kLagFuse = 4;
 constexpr int kLagFullFlag = 1, kLagRunFlag = 2;
+// Accumulator prefetch depth in entries: each consumer thread copies its element's accumulator
+// of entry e + kLagAccSlots into a private shared-memory slot with cp.async while it works on
+// entry e (kLagAccSlots x 8 B per consumer thread; a fused run consumes kLagFuse at once).
+constexpr int kLagAccSlots = 4;
+static_assert(kLagAccSlots >= kLagFuse && (kLagAccSlots & (kLagAccSlots - 1)) == 0, "accumulator ring");
 
 // Geometry of the kernel instantiated for J register frames per element. Up to 32 frames one
 // consumer thread owns an element and holds all J frames in registers; for 64 frames two
@@ -165,6 +173,17 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     return true;
 }
 
+// Per-thread asynchronous 8-byte copy global -> shared (cp.async, the generic proxy) and its
+// group bookkeeping: the accumulator prefetch ring of the consumers.
+__device__ __forceinline__ void cp_async_8(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // |dF|^2 accumulation: the difference as one packed FP32x2 add (sm_100a FADD2, through the
 // compiler's builtin), the squares as two scalar FMAs (measured 11 % faster per launch than a
 // packed FFMA2 on the same chain). With the register frames stored negated, d = b + (-r) is
@@ -222,7 +241,10 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
     unsigned char *smem = smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u);
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + kRingBytes);
     uint64_t *empty = full + kGS;
-    volatile int *abort_flag = reinterpret_cast<volatile int *>(empty + kGS);
+    // accumulator prefetch ring: entry e's value of consumer thread t in accring[(e % kLagAccSlots) * kCT + t]
+    constexpr int kCT = kCW * 32;
+    float2 *accring = reinterpret_cast<float2 *>(empty + kGS);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(accring + kLagAccSlots * kCT);
     volatile int *issued = abort_flag + 1;  // groups the producer has issued (running count)
     int *tab = const_cast<int *>(reinterpret_cast<volatile int *>(abort_flag + 2));
 
@@ -304,14 +326,23 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
                 nr[i] = make_float2(-v.x, -v.y);
             }
             const float2 zero = make_float2(0.f, 0.f);
-            float2 a0 = (valid && ntau > 0) ? acc[static_cast<long long>(ent_acc[0]) * E + k] : zero;
-            float2 a1 = (valid && ntau > 1) ? acc[static_cast<long long>(ent_acc[1]) * E + k] : zero;
-            float2 a2 = (valid && ntau > 2) ? acc[static_cast<long long>(ent_acc[2]) * E + k] : zero;
+            // Accumulator prefetch: one cp.async group per entry, committed in entry order (empty
+            // past the last entry or for an element past E); before entry e is finished, the
+            // groups of entries 0 .. e + kLagAccSlots - 1 are committed. The copies land in shared
+            // memory without holding a register, so the wait before the Kahan step (wait_group)
+            // finds them there kLagAccSlots entries after their issue.
+            float2 *my_acc = accring + tid;
+            auto prefetch_acc = [&](int ee) {
+                if (valid && ee < ntau)
+                    cp_async_8(my_acc + (ee & (kLagAccSlots - 1)) * kCT, acc + static_cast<long long>(ent_acc[ee]) * E + k);
+                cp_async_commit();
+            };
+#pragma unroll
+            for (int ee = 0; ee < kLagAccSlots; ee++) prefetch_acc(ee);
             int waited = 0, released = 0;  // in groups; warp-uniform
             for (int e = 0; e < ntau;) {
                 const int flags = ent_full[e];
                 const int nrun = (flags & kLagRunFlag) ? kLagFuse : 1;  // entries handled in this pass
-                const float2 a3 = (valid && e + 3 < ntau) ? acc[static_cast<long long>(ent_acc[e + 3]) * E + k] : zero;
                 const int ub = ent_ub[e];
                 // Wait for every group this window (or run of windows) reaches that no earlier
                 // window reached; groups without frames included (they complete by the producer's
@@ -326,8 +357,13 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
                         break;
                     }
                 }
-                if (!ok) *abort_flag = 1;
-                if (*abort_flag) break;
+                // A warp leaves on its own failed wait only (no shared flag read per entry): the
+                // others then run out of bounded waits in turn, the producer on the empty barriers
+                // this warp no longer arrives on, the consumers on the groups it no longer issues.
+                if (!ok) {
+                    *abort_flag = 1;
+                    break;
+                }
                 const int s0 = (Gbase * kLagGroup + ub) & (kSlots - 1);  // group G sits in group slot G % kGS
                 // byte offset of this thread's first partner: slot (s0 + j0) of the ring, element m
                 const uint32_t o = static_cast<uint32_t>((s0 + j0) & (kSlots - 1)) * kSlotBytes + toff;
@@ -362,7 +398,10 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
                         sum[r] = c[r].x + c[r].y;
                         if (kLanes == 2) sum[r] += __shfl_xor_sync(0xffffffffu, sum[r], 16);
                     }
-                    float2 ar[kLagFuse] = {a0, a1, a2, a3};
+                    cp_async_wait<kLagAccSlots - kLagFuse>();  // entries e .. e + 3 landed
+                    float2 ar[kLagFuse];
+#pragma unroll
+                    for (int r = 0; r < kLagFuse; r++) ar[r] = my_acc[((e + r) & (kLagAccSlots - 1)) * kCT];
 #pragma unroll
                     for (int r = 0; r < kLagFuse; r++) {
                         const float y = sum[r] - ar[r].y;
@@ -371,9 +410,8 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
                         ar[r].x = t;
                         if (valid && h == 0) acc[static_cast<long long>(ent_acc[e + r]) * E + k] = ar[r];
                     }
-                    a0 = (valid && e + 4 < ntau) ? acc[static_cast<long long>(ent_acc[e + 4]) * E + k] : zero;
-                    a1 = (valid && e + 5 < ntau) ? acc[static_cast<long long>(ent_acc[e + 5]) * E + k] : zero;
-                    a2 = (valid && e + 6 < ntau) ? acc[static_cast<long long>(ent_acc[e + 6]) * E + k] : zero;
+#pragma unroll
+                    for (int r = 0; r < kLagFuse; r++) prefetch_acc(e + kLagAccSlots + r);
                 } else {
                     // one window; four independent packed accumulators (i mod 4) keep the FMA pipeline full
                     float2 acc2[4] = {zero, zero, zero, zero};
@@ -403,14 +441,14 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
                                 ((acc2[2].x + acc2[2].y) + (acc2[3].x + acc2[3].y));
                     if (kLanes == 2) sum += __shfl_xor_sync(0xffffffffu, sum, 16);  // same value in both lanes
                     // Kahan step: a.x running sum, a.y compensation (true value a.x - a.y)
+                    cp_async_wait<kLagAccSlots - 1>();  // entry e landed
+                    float2 a0 = my_acc[(e & (kLagAccSlots - 1)) * kCT];
                     const float y = sum - a0.y;
                     const float t = a0.x + y;
                     a0.y = (t - a0.x) - y;
                     a0.x = t;
                     if (valid && h == 0) acc[static_cast<long long>(ent_acc[e]) * E + k] = a0;
-                    a0 = a1;
-                    a1 = a2;
-                    a2 = a3;
+                    prefetch_acc(e + kLagAccSlots);
                 }
                 e += nrun;
                 // release the groups no later window reads (all their entries lie below the next
@@ -439,6 +477,7 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
                     for (int g = released; g < ngroups; g++) mbar_arrive(&empty[(Gbase + g) & (kGS - 1)]);
             }
         }
+        cp_async_wait<0>();  // a warp that left early may still have accumulator copies in flight
     }
     __syncthreads();
     if (*abort_flag) {
@@ -492,10 +531,11 @@ __global__ void __launch_bounds__(kLagThreads, kLagCtasPerSm)
 }
 
 // Dynamic shared memory of a launch of lag_pipe_kernel<J> with a table of table_ints ints
-// (1 KB of alignment slack, ring, barriers, abort flag, issued-group count, table).
+// (1 KB of alignment slack, ring, barriers, accumulator prefetch ring, abort flag,
+// issued-group count, table).
 inline size_t lag_smem_bytes(int J, int table_ints, int G = 0) {
     return 1024 + static_cast<size_t>(lag_ring_slots(J)) * lag_slot_bytes(J, G) + 2 * sizeof(uint64_t) * lag_group_slots(J) +
-           sizeof(int) * (2 + table_ints);
+           sizeof(float2) * kLagAccSlots * lag_cwarps(G) * 32 + sizeof(int) * (2 + table_ints);
 }
 
 }  // namespace ddm

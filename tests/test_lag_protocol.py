@@ -38,6 +38,7 @@ PROBE = ROOT / "tests" / "_build" / "lag_table_probe"
 # constants of csrc/lag.cuh
 GROUP, CONSUMERS = 8, 4
 FUSE, FULL_FLAG, RUN_FLAG = 4, 1, 2
+ACC_SLOTS = 4
 LAG_JS = (4, 8, 16, 20, 24, 30, 32, 64)
 SMEM_MAX = 220 * 1024
 TAB_ENTRIES = 5 + 64
@@ -200,7 +201,8 @@ def check_table(case: dict, d: dict) -> None:
     assert seen == {u for u in range(nu) if us[u] >= 0}
     ntab = TAB_ENTRIES + 3 * d["ntau"] + nu + d["ngroups"] + 1 + len(d["runs"])
     slots = ring_slots(J)
-    assert 1024 + slots * slot_bytes(J) + 2 * 8 * (slots // GROUP) + 4 * (2 + ntab) <= SMEM_MAX
+    acc_ring = ACC_SLOTS * CONSUMERS * 32 * 8  # accumulator prefetch ring
+    assert 1024 + slots * slot_bytes(J) + 2 * 8 * (slots // GROUP) + acc_ring + 4 * (2 + ntab) <= SMEM_MAX
 
 
 def parity_done(completed: int, parity: int) -> bool:
