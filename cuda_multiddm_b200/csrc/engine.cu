@@ -529,9 +529,9 @@ int check_device_status(ddm_engine *e) {
     int st = 0;
     CUDA_TRY(cudaMemcpyAsync(&st, e->status_d, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
     CUDA_TRY(cudaStreamSynchronize(e->stream));
-    if (st != 0) return fail(DDM_ERR_CUDA, std::string(st == 2 ? "a tensor-core DFT wait" : "a lag-kernel pipeline wait") +
-                                               " timed out (device status " + std::to_string(st) +
-                                               "); results are incomplete");
+    if (st != 0)
+        return fail(DDM_ERR_CUDA, std::string(device_status_text(st)) + " (device status " + std::to_string(st) +
+                                      "); results are incomplete");
     return DDM_OK;
 }
 
@@ -1154,7 +1154,7 @@ static int wait_async_slot(ddm_engine *e, int slot) {
     e->async_pending[slot] = false;
     CUDA_TRY(cudaEventSynchronize(e->async_ev[slot]));
     if (e->async_status_h[slot] != 0)
-        return fail(DDM_ERR_CUDA, "a lag-kernel pipeline wait timed out (device status " +
+        return fail(DDM_ERR_CUDA, std::string(device_status_text(e->async_status_h[slot])) + " (device status " +
                                       std::to_string(e->async_status_h[slot]) + "); results are incomplete");
     return DDM_OK;
 }

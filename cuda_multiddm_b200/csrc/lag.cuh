@@ -162,6 +162,15 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
+// Device status word values (0 = fine): a pipeline wait that ran out, the tensor-core DFT's
+// wait that ran out (csrc/dft_bf16.cuh), a lag kernel whose shared memory was not 1 KB aligned.
+constexpr int kLagStatusWait = 1, kLagStatusDftWait = 2, kLagStatusMisaligned = 3;
+inline const char *device_status_text(int st) {
+    return st == kLagStatusMisaligned ? "the lag kernel's shared memory was not 1 KB aligned"
+           : st == kLagStatusDftWait  ? "a tensor-core DFT wait timed out"
+                                      : "a lag-kernel pipeline wait timed out";
+}
+
 // Bounded wait: false if the phase did not complete within kWaitCycles SM clocks (about
 // 0.2 s at 2 GHz, four orders of magnitude above any legitimate copy latency).
 constexpr long long kWaitCycles = 400000000LL;
@@ -236,9 +245,15 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
     constexpr int kGS = lag_group_slots(J);
     constexpr uint32_t kRingBytes = kSlots * kSlotBytes;
     static_assert(J % kLanes == 0 && (kSlots & (kSlots - 1)) == 0 && (kGS & (kGS - 1)) == 0, "lag geometry");
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
-    // ring slots must start on 1 KB boundaries (TMA destinations): align the base at run time
-    unsigned char *smem = smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u);
+    // Ring slots are TMA destinations and start on 1 KB boundaries: the dynamic shared memory of
+    // a kernel without static shared memory starts on one, so the ring sits at the array's
+    // (link-time constant) address, which every slot address then folds in as an immediate. A
+    // base that is not so aligned is reported (status 3) before anything is copied.
+    extern __shared__ __align__(1024) unsigned char smem[];
+    if (smem_addr(smem) & 1023u) {
+        if (threadIdx.x == 0) atomicExch(status, kLagStatusMisaligned);
+        return;
+    }
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + kRingBytes);
     uint64_t *empty = full + kGS;
     // accumulator prefetch ring: entry e's value of consumer thread t in accring[(e % kLagAccSlots) * kCT + t]
@@ -482,7 +497,7 @@ __device__ __forceinline__ void lag_pipe_body(const float2 *__restrict__ ring, f
     __syncthreads();
     if (*abort_flag) {
         if (tid == 0) {
-            atomicExch(status, 1);
+            atomicExch(status, kLagStatusWait);
             // drain: wait (bounded) until every copy this CTA issued has landed; a group slot
             // holds at most one fill in flight, its latest
             const int n = *issued;
@@ -531,10 +546,9 @@ __global__ void __launch_bounds__(kLagThreads, kLagCtasPerSm)
 }
 
 // Dynamic shared memory of a launch of lag_pipe_kernel<J> with a table of table_ints ints
-// (1 KB of alignment slack, ring, barriers, accumulator prefetch ring, abort flag,
-// issued-group count, table).
+// (ring, barriers, accumulator prefetch ring, abort flag, issued-group count, table).
 inline size_t lag_smem_bytes(int J, int table_ints, int G = 0) {
-    return 1024 + static_cast<size_t>(lag_ring_slots(J)) * lag_slot_bytes(J, G) + 2 * sizeof(uint64_t) * lag_group_slots(J) +
+    return static_cast<size_t>(lag_ring_slots(J)) * lag_slot_bytes(J, G) + 2 * sizeof(uint64_t) * lag_group_slots(J) +
            sizeof(float2) * kLagAccSlots * lag_cwarps(G) * 32 + sizeof(int) * (2 + table_ints);
 }
 

@@ -203,6 +203,8 @@ extern "C" int ddm_lag_accumulate_static(const void *ring, int ring_slots, long 
     const cudaError_t se = cudaStreamSynchronize(s);
     if (ce == cudaSuccess) ce = se;
     if (ce != cudaSuccess) return fail(DDM_ERR_CUDA, std::string("ddm_lag_accumulate_static: ") + cudaGetErrorString(ce));
-    if (status != 0) return fail(DDM_ERR_CUDA, "ddm_lag_accumulate_static: a pipeline wait timed out; accumulators incomplete");
+    if (status != 0)
+        return fail(DDM_ERR_CUDA, std::string("ddm_lag_accumulate_static: ") + device_status_text(status) +
+                                      "; accumulators incomplete");
     return DDM_OK;
 }

@@ -535,7 +535,8 @@ extern "C" int ddm_server_poll(ddm_server *s, int stream_id, ddm_chunk_result *r
     Stream &st = it->second;
     if (st.order.empty() || st.order.front()->state.load() != 2) return 0;
     Slot *slot = st.order.front();
-    if (*slot->status_h != 0) return fail(DDM_ERR_CUDA, "a lag-kernel pipeline wait timed out; results are incomplete");
+    if (*slot->status_h != 0)
+        return fail(DDM_ERR_CUDA, std::string(device_status_text(*slot->status_h)) + "; results are incomplete");
     if (isf) {
         if (capacity < st.isf_size) return fail(DDM_ERR_INVALID_ARG, "ddm_server_poll: ISF buffer too small");
         std::memcpy(isf, slot->isf_h, sizeof(double) * st.isf_size);

@@ -21,6 +21,7 @@ start|end windows (src/DDM.cu:250-255) — plus random windows with holes, and c
 """
 from __future__ import annotations
 
+import os
 import random
 import subprocess
 import sys
@@ -61,8 +62,12 @@ def probe() -> Path:
     deps = [PROBE_SRC, CSRC / "lag_host.hpp", CSRC / "lag.cuh"]
     if not PROBE.exists() or PROBE.stat().st_mtime < max(p.stat().st_mtime for p in deps):
         PROBE.parent.mkdir(parents=True, exist_ok=True)
+        # built under a private name and renamed into place, so parallel test workers never
+        # run a half-written binary
+        tmp = PROBE.with_name(f"{PROBE.name}.{os.getpid()}")
         subprocess.run(["nvcc", "-std=c++17", "-O1", "-gencode", "arch=compute_100a,code=sm_100a",
-                        "-I", str(CSRC), str(PROBE_SRC), "-o", str(PROBE)], check=True)
+                        "-I", str(CSRC), str(PROBE_SRC), "-o", str(tmp)], check=True)
+        os.replace(tmp, PROBE)
     return PROBE
 
 
@@ -202,7 +207,7 @@ def check_table(case: dict, d: dict) -> None:
     ntab = TAB_ENTRIES + 3 * d["ntau"] + nu + d["ngroups"] + 1 + len(d["runs"])
     slots = ring_slots(J)
     acc_ring = ACC_SLOTS * CONSUMERS * 32 * 8  # accumulator prefetch ring
-    assert 1024 + slots * slot_bytes(J) + 2 * 8 * (slots // GROUP) + acc_ring + 4 * (2 + ntab) <= SMEM_MAX
+    assert slots * slot_bytes(J) + 2 * 8 * (slots // GROUP) + acc_ring + 4 * (2 + ntab) <= SMEM_MAX
 
 
 def parity_done(completed: int, parity: int) -> bool:
