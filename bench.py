@@ -320,7 +320,7 @@ def run_ours(args, w: dict) -> None:
                        tolerance=1.2, chunk_frames=CHUNK, estimator="unbiased", device=local,
                        lag_batch_frames=args.lag_batch, bytes_per_pixel=bpp, pixel_mode=w["pixel_mode"],
                        lag_geometry=args.lag_geometry, small_tile_dft=args.small_tile_dft,
-                       fft_per_tile=args.fft_per_tile)
+                       fft_per_tile=args.fft_per_tile, fft_group_frames=args.fft_group)
     eng = Engine(cfg)
     stream = torch.cuda.ExternalStream(eng.info().stream)
     preroll = math.ceil(max(taus) / CHUNK) + 1
@@ -418,6 +418,7 @@ def run_ours(args, w: dict) -> None:
                 "impl_config": {"lag_batch_frames": eng.info().lag_batch_frames,
                                 "lag_geometry": args.lag_geometry, "small_tile_dft": bool(args.small_tile_dft),
                                 "fft_per_tile": bool(args.fft_per_tile),
+                                "fft_group_frames": eng.info().fft_group_frames,
                                 "ring_slots": eng.info().ring_slots,
                                 "frame_spectra_mb": frames_elements(w) * 8 / 1e6},
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": CHUNK * side * side * bpp,
@@ -497,6 +498,8 @@ def main() -> None:
                     help="split-BF16 tensor-core DFT for tiles of side 32..128 instead of the FP32 FFT")
     ap.add_argument("--fft-per-tile", action="store_true",
                     help="tiles of side 32..128 through the per-tile FFT kernel (default: two passes for every scale)")
+    ap.add_argument("--fft-group", type=int, default=0,
+                    help="frames per FFT launch (0 = the engine default: as many as 256 MB of spectra hold)")
     ap.add_argument("--workload", choices=["c1", "c2", "c3", "c4", "multiscale", "small", "serving"], default="c2",
                     help="c2 (default): the headline 1024^2 x 4-scale x 64-tau workload; c1, c3, c4: the other "
                          "configurations; small: 512^2 frames with c2's taus (profiling only); serving: many "
