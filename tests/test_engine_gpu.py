@@ -170,6 +170,30 @@ def test_full_lag_launches_match_oracle():
     assert_isf_close(live, isf, scales, len(lambdas), len(taus), rtol=2e-6)
 
 
+def test_large_pair_table_two_ctas_per_sm_matches_oracle():
+    """Taus 40 frames apart (48 of them, up to 1881) share no partner frames, so a 32-frame
+    launch's union holds 1536 of them and its pair table needs over 8 KB: a lag CTA then takes
+    more than 76.8 KB of shared memory, two fit on an SM instead of three, and the persistent
+    grid (sized by the occupancy API) is two CTAs per SM walking the 518 element blocks of
+    256^2 frames at scales 256 and 128. Early launches have partial windows (frames without
+    all their partners yet), later ones full windows."""
+    taus = [1 + 40 * i for i in range(48)]
+    frames = media.synth_video(57, 256, 256, 1900, 200, step_var=1.0)
+    scales, lambdas = [256, 128], [3.0, 8.0, 20.0, 60.0]
+    # lower bound of a full 32-frame launch's shared memory (ring, barriers, accumulator ring,
+    # flags, table with at least one run per group), against what three CTAs per SM allow
+    J, T = 32, len(taus)
+    union = len({w + j for w in (max(taus) - t for t in taus) for j in range(J)})
+    groups = (union + 7) // 8
+    table_ints = 5 + 64 + 3 * T + union + groups + 1 + groups
+    smem = 64 * 1024 + 2 * 8 * 8 + 4 * 4 * 32 * 8 + 4 * (2 + table_ints)
+    assert union == T * J and 3 * (smem + 1024) > 228 * 1024 and 2 * (smem + 1024) <= 228 * 1024
+    isf, _, info = engine_run(frames, scales, taus, lambdas, estimator="unbiased", C=30)
+    assert info.lag_batch_frames == 32
+    want, _ = O.ddm_run(frames, scales, taus, lambdas, estimator=O.EST_UNBIASED, chunk=30)
+    assert_isf_close(isf, want, scales, len(lambdas), len(taus))
+
+
 def test_lag_batch_sizes_agree():
     """The same stream paired in launches of 1, 13, 30 and 64 frames gives the same ISF."""
     frames = media.synth_video(44, 64, 64, 90, 30, step_var=1.0)
