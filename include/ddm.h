@@ -325,7 +325,9 @@ void ddm_host_free(void *ptr);
  * above any legitimate copy latency). A wait that runs out makes the kernel finish its copies
  * in flight and return with a device status that the next ddm_finalize, ddm_synchronize or
  * ddm_wait_isf reports as DDM_ERR_CUDA ("... wait timed out ..."); the CUDA context stays
- * usable. The reference has no such path: every error there ends the process
+ * usable. The same report, worded "... shared memory was not 1 KB aligned", comes from a lag
+ * kernel that found its dynamic shared memory off a 1 KB boundary: it returns before
+ * issuing any copy. The reference has no such path: every error there ends the process
  * (src/debug.cpp:10-15). */
 int ddm_set_wait_limit(ddm_engine *e, long long cycles);
 
