@@ -181,6 +181,8 @@ struct ddm_engine {
     // kernel timing (ddm_set_timing): event pairs and launch counts per kernel group
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> tev[3];
+    std::vector<cudaEvent_t> tev_pool;  // read-out timing events, reused (creating them per
+                                        // range made a small workload's steps host-bound)
     long tlaunch[3] = {0, 0, 0};
     // compulsory DRAM bytes of the kernels launched since the last ddm_kernel_stats: what
     // each kernel must move at least (its inputs read once, its outputs written once)
@@ -240,6 +242,7 @@ void free_all(ddm_engine *e) {
             cudaEventDestroy(pr.first);
             cudaEventDestroy(pr.second);
         }
+    for (cudaEvent_t ev : e->tev_pool) cudaEventDestroy(ev);
     if (e->ev_fft) cudaEventDestroy(e->ev_fft);
     if (e->ev_copy) cudaEventDestroy(e->ev_copy);
     if (e->ev_stage) cudaEventDestroy(e->ev_stage);
@@ -255,23 +258,38 @@ void free_all(ddm_engine *e) {
 }
 
 // Brackets a group of launches with events when timing is on (group 0 FFT, 1 lag, 2 azimuth).
+// A timing event from the engine's pool (created when the pool is empty; nullptr on failure).
+inline cudaEvent_t timing_event(ddm_engine *e) {
+    if (!e->tev_pool.empty()) {
+        cudaEvent_t ev = e->tev_pool.back();
+        e->tev_pool.pop_back();
+        return ev;
+    }
+    cudaEvent_t ev = nullptr;
+    return cudaEventCreate(&ev) == cudaSuccess ? ev : nullptr;
+}
+
 struct TimedRange {
     ddm_engine *e;
     int group;
     cudaStream_t stream;
     cudaEvent_t start = nullptr;
     TimedRange(ddm_engine *e_, int g) : e(e_), group(g), stream(g == 0 ? e_->fft_stream : e_->stream) {
-        if (e->timing && cudaEventCreate(&start) == cudaSuccess) cudaEventRecord(start, stream);
+        if (e->timing && (start = timing_event(e))) cudaEventRecord(start, stream);
     }
+    ~TimedRange() {  // a range left on an error path gives its event back
+        if (start) e->tev_pool.push_back(start);
+    }
+    TimedRange(const TimedRange &) = delete;
+    TimedRange &operator=(const TimedRange &) = delete;
     void end(long launches) {
         e->tlaunch[group] += launches;
         if (!start) return;
-        cudaEvent_t stop;
-        if (cudaEventCreate(&stop) == cudaSuccess) {
+        if (cudaEvent_t stop = timing_event(e)) {
             cudaEventRecord(stop, stream);
             e->tev[group].push_back({start, stop});
         } else {
-            cudaEventDestroy(start);
+            e->tev_pool.push_back(start);
         }
         start = nullptr;
     }
@@ -1448,8 +1466,8 @@ extern "C" int ddm_kernel_stats(ddm_engine *e, double *ms, long *launches, doubl
         for (auto &pr : e->tev[g]) {
             float t = 0.f;
             if (cudaEventElapsedTime(&t, pr.first, pr.second) == cudaSuccess) total += t;
-            cudaEventDestroy(pr.first);
-            cudaEventDestroy(pr.second);
+            e->tev_pool.push_back(pr.first);
+            e->tev_pool.push_back(pr.second);
         }
         e->tev[g].clear();
         ms[g] = total;
