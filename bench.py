@@ -25,7 +25,9 @@ timed region ends with the azimuthal average (ISF ready).
 
   value    frames/s with the video resident in HBM (device pointers submitted)
   e2e      frames/s through the public API from pinned host memory: every step copies its
-           30 frames host->device and reads the updated ISF (a live result) device->host
+           30 frames host->device and reads the updated ISF (a live result) device->host,
+           three results in flight (ddm_set_async_depth(4)); the region ends with the last
+           result in host memory
   roofline the lag kernel against HBM: achieved = the compulsory DRAM bytes of its launches
            (each register frame and each distinct partner frame of a launch read once, each
            accumulator row read and written once; counted by the engine) / their CUDA-event
@@ -56,6 +58,7 @@ sys.path.insert(0, str(ROOT))
 
 UNIT = "frames/s"
 CHUNK = 30
+ASYNC_DEPTH = 4  # e2e: live results in flight + 1 (ddm_set_async_depth)
 
 
 def log_taus(lo: int, hi: int, n: int) -> list[int]:
@@ -366,17 +369,18 @@ def run_ours(args, w: dict) -> None:
 
     # ---- end to end from pinned host memory ---------------------------------------
     # Every step copies its chunk from pinned host memory and reads back the ISF of the
-    # stream so far (ddm_finalize_async into one of two pinned buffers); the next chunk is
-    # submitted while that result is on its way, and the region ends once the last one is in
-    # host memory.
+    # stream so far (ddm_finalize_async into one of ASYNC_DEPTH pinned buffers, ASYNC_DEPTH - 1
+    # results in flight); the next chunks are submitted while earlier results are on their
+    # way, and the region ends once the last one is in host memory.
     eng.set_timing(False)
-    isf_bufs = [eng.pinned_isf_buffer() for _ in range(2)]
+    eng.set_async_depth(ASYNC_DEPTH)
+    isf_bufs = [eng.pinned_isf_buffer() for _ in range(ASYNC_DEPTH)]
     step_no = [0]
 
     def step_host():
         i = next_chunk()
         eng.submit(host_video[i:i + CHUNK].data_ptr(), CHUNK, False)
-        eng.finalize_async(isf_bufs[step_no[0] % 2])
+        eng.finalize_async(isf_bufs[step_no[0] % ASYNC_DEPTH])
         step_no[0] += 1
 
     for _ in range(args.warmup):
@@ -419,6 +423,7 @@ def run_ours(args, w: dict) -> None:
                                 "lag_geometry": args.lag_geometry, "small_tile_dft": bool(args.small_tile_dft),
                                 "fft_per_tile": bool(args.fft_per_tile),
                                 "fft_group_frames": eng.info().fft_group_frames,
+                                "e2e_results_in_flight": ASYNC_DEPTH - 1,
                                 "ring_slots": eng.info().ring_slots,
                                 "frame_spectra_mb": frames_elements(w) * 8 / 1e6},
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": CHUNK * side * side * bpp,

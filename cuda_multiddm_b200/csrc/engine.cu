@@ -56,6 +56,7 @@ using namespace ddm;
 namespace {
 
 constexpr int kTables = 64;  // lag tables in flight
+constexpr int kAsyncMax = 8;  // ddm_finalize_async result slots (ddm_set_async_depth)
 
 struct Launch {  // one lag-kernel launch: register frames, tau windows (ascending), position slots
     int nreg = 0;
@@ -139,10 +140,11 @@ struct ddm_engine {
     int norm_slot = 0;
     // ddm_finalize_async results alternate between two slots: the status word copied with
     // the result, the event after both copies, and whether it has been waited for
-    int *async_status_h = nullptr;           // pinned, 2 ints
-    cudaEvent_t async_ev[2] = {nullptr, nullptr};
-    bool async_pending[2] = {false, false};
+    int *async_status_h = nullptr;           // pinned, kAsyncMax ints
+    cudaEvent_t async_ev[kAsyncMax] = {};
+    bool async_pending[kAsyncMax] = {};
     int async_slot = 0;                      // slot of the next result
+    int async_depth = 2;                     // result slots in use (ddm_set_async_depth)
     // their copies run on result_stream, so the next chunk's lag work does not queue behind
     // them; ev_isf_ready orders a copy after its azimuthal average, ev_isf_read holds the
     // next azimuthal average (which rewrites isf_d) until the copy has read it
@@ -230,8 +232,9 @@ void free_all(ddm_engine *e) {
     for (int i = 0; i < 2; i++) {
         if (e->norm_ev[i]) cudaEventDestroy(e->norm_ev[i]);
         if (e->norm_free[i]) cudaEventDestroy(e->norm_free[i]);
-        if (e->async_ev[i]) cudaEventDestroy(e->async_ev[i]);
     }
+    for (int i = 0; i < kAsyncMax; i++)
+        if (e->async_ev[i]) cudaEventDestroy(e->async_ev[i]);
     pinned_release(e->tables_h);
     for (int i = 0; i < kTables; i++) {
         if (e->tab_ev[i]) cudaEventDestroy(e->tab_ev[i]);
@@ -900,12 +903,14 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
     if ((st = dev_alloc(e, &e->status_d, 1))) return bail(st);
     if (cudaMemset(e->status_d, 0, sizeof(int)) != cudaSuccess) return bail(fail(DDM_ERR_CUDA, "status memset failed"));
     e->norm_h = static_cast<double *>(pinned_alloc(sizeof(double) * 2 * e->T));
-    e->async_status_h = static_cast<int *>(pinned_alloc(sizeof(int) * 2));
+    e->async_status_h = static_cast<int *>(pinned_alloc(sizeof(int) * kAsyncMax));
     if (!e->norm_h || !e->async_status_h) return bail(fail(DDM_ERR_OUT_OF_MEMORY, "pinned norm and status buffers"));
     for (int i = 0; i < 2; i++)
         if (cudaEventCreateWithFlags(&e->norm_ev[i], cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&e->norm_free[i], cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&e->async_ev[i], cudaEventDisableTiming) != cudaSuccess)
+            cudaEventCreateWithFlags(&e->norm_free[i], cudaEventDisableTiming) != cudaSuccess)
+            return bail(fail(DDM_ERR_CUDA, "cudaEventCreate failed"));
+    for (int i = 0; i < kAsyncMax; i++)
+        if (cudaEventCreateWithFlags(&e->async_ev[i], cudaEventDisableTiming) != cudaSuccess)
             return bail(fail(DDM_ERR_CUDA, "cudaEventCreate failed"));
     e->tables_h = static_cast<int *>(pinned_alloc(sizeof(int) * static_cast<size_t>(kTables) * e->tab_stride));
     if (!e->tables_h) return bail(fail(DDM_ERR_OUT_OF_MEMORY, "pinned table buffer"));
@@ -1075,6 +1080,18 @@ extern "C" int ddm_submit_frames(ddm_engine *e, const void *frames, int count, i
             const size_t roi_row = static_cast<size_t>(e->M) * e->bpp;
             if (e->stage_busy) CUDA_TRY(cudaStreamWaitEvent(e->copy_stream, e->ev_stage, 0));
             auto copy_group = [&](int f0, int nf) -> int {
+                if (e->M == e->h) {
+                    // the ROI spans the frame's height: the rows of consecutive frames are
+                    // evenly strided in the packed buffer, so the group is one 2-D copy
+                    const uint8_t *fp = p + frame_bytes * f0 + static_cast<size_t>(e->x_off) * e->bpp;
+                    CUDA_TRY(cudaMemcpy2DAsync(e->stage + static_cast<size_t>(f0) * e->M * roi_row, roi_row, fp,
+                                               static_cast<size_t>(e->w) * e->bpp, roi_row,
+                                               static_cast<size_t>(e->M) * nf, cudaMemcpyHostToDevice,
+                                               e->copy_stream));
+                    CUDA_TRY(cudaEventRecord(e->ev_copy, e->copy_stream));
+                    CUDA_TRY(cudaStreamWaitEvent(e->fft_stream, e->ev_copy, 0));
+                    return DDM_OK;
+                }
                 for (int f = f0; f < f0 + nf; f++) {
                     const uint8_t *fp = p + frame_bytes * f +
                                         (static_cast<size_t>(e->y_off) * e->w + e->x_off) * e->bpp;
@@ -1181,7 +1198,7 @@ extern "C" int ddm_finalize_async(ddm_engine *e, double *out, long capacity) {
     clear_error();
     if (!e || !out || capacity < e->isf_size) return fail(DDM_ERR_INVALID_ARG, "ddm_finalize_async: bad argument");
     const int slot = e->async_slot;
-    int st = wait_async_slot(e, slot);  // two results ago: already waited for by the call after it
+    int st = wait_async_slot(e, slot);  // async_depth results ago: already waited for by the call after it
     if (st) return st;
     // queue this result first, so the stream never idles while the host waits below
     if ((st = engine_finalize_async(e))) return st;
@@ -1193,17 +1210,33 @@ extern "C" int ddm_finalize_async(ddm_engine *e, double *out, long capacity) {
     CUDA_TRY(cudaEventRecord(e->async_ev[slot], e->result_stream));
     CUDA_TRY(cudaEventRecord(e->ev_isf_read, e->result_stream));
     e->async_pending[slot] = true;
-    e->async_slot = slot ^ 1;
-    return wait_async_slot(e, slot ^ 1);  // the previous result: its buffer is the caller's again
+    e->async_slot = (slot + 1) % e->async_depth;
+    // the result of async_depth - 1 calls ago (the previous one at the default depth of 2):
+    // its buffer is the caller's again
+    return wait_async_slot(e, e->async_slot);
+}
+
+extern "C" int ddm_set_async_depth(ddm_engine *e, int depth) {
+    clear_error();
+    if (!e || depth < 2 || depth > kAsyncMax)
+        return fail(DDM_ERR_INVALID_ARG, "ddm_set_async_depth: depth must be 2.." + std::to_string(kAsyncMax));
+    for (int i = 0; i < kAsyncMax; i++)
+        if (e->async_pending[i]) return fail(DDM_ERR_STATE, "ddm_set_async_depth: results still in flight (ddm_wait_isf)");
+    e->async_depth = depth;
+    e->async_slot = 0;
+    return DDM_OK;
 }
 
 extern "C" int ddm_wait_isf(ddm_engine *e) {
     clear_error();
     if (!e) return fail(DDM_ERR_INVALID_ARG, "ddm_wait_isf: null engine");
-    const int older = e->async_slot;  // the slot of the next result holds the older one, if any
-    int st = wait_async_slot(e, older);
-    int st2 = wait_async_slot(e, older ^ 1);
-    return st ? st : st2;
+    // oldest first: the slot of the next result holds the oldest one in flight, if any
+    int st = DDM_OK;
+    for (int i = 0; i < e->async_depth; i++) {
+        const int s2 = wait_async_slot(e, (e->async_slot + i) % e->async_depth);
+        if (!st) st = s2;
+    }
+    return st;
 }
 
 extern "C" int ddm_read_isf(ddm_engine *e, double *out, long capacity) {

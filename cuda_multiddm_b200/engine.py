@@ -157,6 +157,12 @@ class Engine:
     def wait_isf(self) -> None:
         check(lib().ddm_wait_isf(self._h))
 
+    def set_async_depth(self, depth: int) -> None:
+        """Keep depth - 1 finalize_async results in flight (2..8; default 2): each call then
+        returns once the result of depth - 1 calls before is in its buffer, so the caller
+        cycles `depth` buffers. Only with no result in flight (after wait_isf)."""
+        check(lib().ddm_set_async_depth(self._h, int(depth)))
+
     def pinned_isf_buffer(self) -> np.ndarray:
         """A page-locked float64 buffer of isf_size values (the array keeps its pinned
         tensor alive)."""

@@ -153,6 +153,12 @@ int ddm_read_isf(ddm_engine *e, double *isf_out, long capacity);
  * times; compat: once, as ddm_finalize. */
 int ddm_finalize_async(ddm_engine *e, double *isf_out, long capacity);
 
+/* Results ddm_finalize_async keeps in flight: with depth d (2..8, default 2) the call queues
+ * its result and waits for the one of d - 1 calls before, so a caller cycles d buffers and d - 1
+ * results are on their way at any time (for chunks whose GPU work is shorter than a result's
+ * round trip). Only between results: DDM_ERR_STATE while any is in flight (ddm_wait_isf). */
+int ddm_set_async_depth(ddm_engine *e, int depth);
+
 /* Block until the last ddm_finalize_async result is in its buffer; returns DDM_ERR_CUDA if
  * a kernel queued before it reported a failure (the status ddm_finalize checks). */
 int ddm_wait_isf(ddm_engine *e);

@@ -269,6 +269,46 @@ def test_finalize_async_matches_finalize():
             assert lib().ddm_finalize_async(eng._h, short.ctypes.data, eng.isf_size - 1) == 1  # DDM_ERR_INVALID_ARG
 
 
+@pytest.mark.parametrize("depth", [3, 4, 8])
+def test_finalize_async_depth_matches_finalize(depth):
+    """With ddm_set_async_depth(d), d - 1 results stay in flight: finalize_async(k) returns
+    once result k - d + 1 is in its buffer (the caller cycles d buffers), and every result
+    equals ddm_finalize + ddm_read_isf after the same chunk bit for bit; the depth can change
+    only with nothing in flight."""
+    frames = media.synth_video(49, 128, 128, 150, 40, step_var=1.0)
+    kw = dict(frame_width=128, frame_height=128, scales=[128, 64], taus=[1, 2, 3, 4, 7, 12, 25],
+              lambdas=[3.0, 6.0, 12.0, 24.0], chunk_frames=15, estimator="unbiased")
+    n = 150 // 15
+    with Engine(EngineConfig(**kw)) as eng:
+        want = []
+        for c0 in range(0, 150, 15):
+            eng.submit(frames[c0:c0 + 15])
+            eng.finalize()
+            want.append(eng.isf())
+    with Engine(EngineConfig(**kw)) as eng:
+        eng.set_async_depth(depth)
+        bufs = [eng.pinned_isf_buffer() for _ in range(depth)]
+        got = {}
+        for k in range(n):
+            eng.submit(frames[15 * k:15 * k + 15])
+            eng.finalize_async(bufs[k % depth])
+            if k - depth + 1 >= 0:
+                got[k - depth + 1] = bufs[(k - depth + 1) % depth].copy()
+            if k == 1:
+                with pytest.raises(DDMError):  # results in flight
+                    eng.set_async_depth(2)
+        eng.wait_isf()
+        for j in range(max(0, n - depth + 1), n):
+            got[j] = bufs[j % depth].copy()
+        assert sorted(got) == list(range(n))
+        for j in range(n):
+            assert np.array_equal(got[j], want[j]), j
+        eng.set_async_depth(2)  # nothing in flight now
+        for bad in (1, 9):
+            with pytest.raises(DDMError):
+                eng.set_async_depth(bad)
+
+
 def test_compat_long_chunk_matches_oracle():
     """C = 100 with lag_batch_frames = 64: each reference iteration pairs 100 A-frames, run as
     a 64-frame launch and a 36-frame launch of the 64-frame kernel (the partial-window path);
