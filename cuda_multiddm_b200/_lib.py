@@ -87,6 +87,7 @@ SIGNATURES = {
     "ddm_tune_key": (C.c_long, [C.POINTER(Config), C.c_char_p, C.c_long]),
     "ddm_wait_isf": (C.c_int, [C.c_void_p]),
     "ddm_set_async_depth": (C.c_int, [C.c_void_p, C.c_int]),
+    "ddm_wait_frames_copied": (C.c_int, [C.c_void_p, C.c_int]),
     "ddm_dump_count": (C.c_int, [C.c_void_p]),
     "ddm_read_dump": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_long]),
     "ddm_reset_accumulators": (C.c_int, [C.c_void_p]),

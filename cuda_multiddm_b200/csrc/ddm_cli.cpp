@@ -412,15 +412,42 @@ int main(int argc, char **argv) {
     int which = 0;
     PowerWriter power;
     std::vector<float> pw(power_out ? ddm_frame_elements(eng) : 0);
-    while (sent < frames_total) {
-        const int n = static_cast<int>(std::min<long>(chunk, frames_total - sent));
+    auto read_chunk = [&](int n) {
         if (!bench && ddm_movie_read(mv, buf[which], n) != DDM_OK) {
             std::fprintf(stderr, "%s\n", ddm_last_error());
-            return EXIT_FAILURE;
+            std::exit(EXIT_FAILURE);
         }
-        if (!power_out) {
+    };
+    auto write_dumps = [&]() {
+        while (dumps_written < ddm_dump_count(eng)) {  // -G snapshots, src/DDM.cu:800-826
+            if (ddm_read_dump(eng, dumps_written, isf.data(), static_cast<long>(isf.size())) != DDM_OK)
+                die(ddm_last_error());
+            write_all(file_out + "_t" + std::to_string(dumps_written) + "_");
+            dumps_written++;
+        }
+    };
+    if (!power_out) {
+        // Two buffers: chunk k+1 is read from the file while the engine transforms and pairs
+        // chunk k; before a buffer is refilled, the copies of the submit call before last (its
+        // frames) must have finished.
+        int n = static_cast<int>(std::min<long>(chunk, frames_total));
+        read_chunk(n);
+        while (sent < frames_total) {
             if (ddm_submit_frames(eng, buf[which], n, 0) != DDM_OK) die(ddm_last_error());
-        } else {
+            sent += n;
+            which ^= 1;
+            write_dumps();
+            verbose("[Chunk complete]%s\n");
+            if (sent < frames_total) {
+                n = static_cast<int>(std::min<long>(chunk, frames_total - sent));
+                if (!bench && ddm_wait_frames_copied(eng, 1) != DDM_OK) die(ddm_last_error());
+                read_chunk(n);
+            }
+        }
+    } else {
+        while (sent < frames_total) {
+            const int n = static_cast<int>(std::min<long>(chunk, frames_total - sent));
+            read_chunk(n);
             // -A: submit in pieces no larger than the engine's ingest piece (min(C, 32) frames;
             // the ring holds at least that many latest frames), reading each piece's spectra
             power.open(file_out, sent / chunk, scales);
@@ -438,19 +465,11 @@ int main(int argc, char **argv) {
                 }
             }
             power.close();
+            sent += n;
+            which ^= 1;
+            write_dumps();
+            verbose("[Chunk complete]%s\n");
         }
-        sent += n;
-        which ^= 1;
-        // the other buffer is refilled next: its copy must have finished (benchmark mode
-        // never refills its buffers)
-        if (!bench && ddm_synchronize(eng) != DDM_OK) die(ddm_last_error());
-        while (dumps_written < ddm_dump_count(eng)) {  // -G snapshots, src/DDM.cu:800-826
-            if (ddm_read_dump(eng, dumps_written, isf.data(), static_cast<long>(isf.size())) != DDM_OK)
-                die(ddm_last_error());
-            write_all(file_out + "_t" + std::to_string(dumps_written) + "_");
-            dumps_written++;
-        }
-        verbose("[Chunk complete]%s\n");
     }
     if (ddm_synchronize(eng) != DDM_OK) die(ddm_last_error());
     auto t_main = std::chrono::high_resolution_clock::now();

@@ -57,6 +57,7 @@ namespace {
 
 constexpr int kTables = 64;  // lag tables in flight
 constexpr int kAsyncMax = 8;  // ddm_finalize_async result slots (ddm_set_async_depth)
+constexpr int kSubmitEvents = 8;  // submit calls ddm_wait_frames_copied can look back over
 
 struct Launch {  // one lag-kernel launch: register frames, tau windows (ascending), position slots
     int nreg = 0;
@@ -145,6 +146,9 @@ struct ddm_engine {
     bool async_pending[kAsyncMax] = {};
     int async_slot = 0;                      // slot of the next result
     int async_depth = 2;                     // result slots in use (ddm_set_async_depth)
+    // copy stream: the host frames of each of the last kSubmitEvents submit calls have been read
+    cudaEvent_t submit_ev[kSubmitEvents] = {};
+    long long submit_calls = 0;
     // their copies run on result_stream, so the next chunk's lag work does not queue behind
     // them; ev_isf_ready orders a copy after its azimuthal average, ev_isf_read holds the
     // next azimuthal average (which rewrites isf_d) until the copy has read it
@@ -235,6 +239,8 @@ void free_all(ddm_engine *e) {
     }
     for (int i = 0; i < kAsyncMax; i++)
         if (e->async_ev[i]) cudaEventDestroy(e->async_ev[i]);
+    for (int i = 0; i < kSubmitEvents; i++)
+        if (e->submit_ev[i]) cudaEventDestroy(e->submit_ev[i]);
     pinned_release(e->tables_h);
     for (int i = 0; i < kTables; i++) {
         if (e->tab_ev[i]) cudaEventDestroy(e->tab_ev[i]);
@@ -912,6 +918,9 @@ int open_engine(const ddm_config *cfg, ddm_engine **out, size_t *need_out, bool 
     for (int i = 0; i < kAsyncMax; i++)
         if (cudaEventCreateWithFlags(&e->async_ev[i], cudaEventDisableTiming) != cudaSuccess)
             return bail(fail(DDM_ERR_CUDA, "cudaEventCreate failed"));
+    for (int i = 0; i < kSubmitEvents; i++)
+        if (cudaEventCreateWithFlags(&e->submit_ev[i], cudaEventDisableTiming) != cudaSuccess)
+            return bail(fail(DDM_ERR_CUDA, "cudaEventCreate failed"));
     e->tables_h = static_cast<int *>(pinned_alloc(sizeof(int) * static_cast<size_t>(kTables) * e->tab_stride));
     if (!e->tables_h) return bail(fail(DDM_ERR_OUT_OF_MEMORY, "pinned table buffer"));
     for (int i = 0; i < kTables; i++)
@@ -1129,6 +1138,18 @@ extern "C" int ddm_submit_frames(ddm_engine *e, const void *frames, int count, i
         }
         done += piece;
     }
+    // every copy of this call's host frames is queued on the copy stream by now
+    CUDA_TRY(cudaEventRecord(e->submit_ev[e->submit_calls % kSubmitEvents], e->copy_stream));
+    e->submit_calls++;
+    return DDM_OK;
+}
+
+extern "C" int ddm_wait_frames_copied(ddm_engine *e, int back) {
+    clear_error();
+    if (!e || back < 0 || back >= kSubmitEvents)
+        return fail(DDM_ERR_INVALID_ARG, "ddm_wait_frames_copied: back must be 0.." + std::to_string(kSubmitEvents - 1));
+    if (back >= e->submit_calls) return DDM_OK;  // no such call
+    CUDA_TRY(cudaEventSynchronize(e->submit_ev[(e->submit_calls - 1 - back) % kSubmitEvents]));
     return DDM_OK;
 }
 

@@ -6,6 +6,9 @@
 // camera type, pixel mode, header length, data length}; the full header is 172 bytes
 // (IIDC), 128 (Andor) or 240 (Ximea). Frame size and the timestamp used for the frame
 // rate sit at fixed offsets in those headers (read below as little-endian fields).
+#include <unistd.h>
+
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -57,6 +60,7 @@ struct ddm_movie {
     int header_len = 0;
     uint32_t length_data = 0;
     int w = 0, h = 0, bpp = 1;
+    long long pos = 0;  // file offset of the next frame's header
 };
 
 extern "C" int ddm_movie_open(const char *path, int frame_offset, ddm_movie **out,
@@ -105,6 +109,7 @@ extern "C" int ddm_movie_open(const char *path, int frame_offset, ddm_movie **ou
 
     ddm_movie *m = new ddm_movie;
     m->f = f;
+    m->pos = magic_offset + static_cast<long long>(frame_offset) * (hl + static_cast<long long>(length_data));
     m->type = type;
     m->header_len = hl;
     m->length_data = length_data;
@@ -129,18 +134,54 @@ extern "C" int ddm_movie_open(const char *path, int frame_offset, ddm_movie **ou
     return DDM_OK;
 }
 
+namespace {
+// All `n` bytes at file offset `at`, in as many positioned reads as the system returns.
+bool read_at(int fd, void *dst, size_t n, long long at) {
+    unsigned char *p = static_cast<unsigned char *>(dst);
+    while (n > 0) {
+        const ssize_t r = ::pread(fd, p, n, static_cast<off_t>(at));
+        if (r <= 0) return false;
+        p += r;
+        at += r;
+        n -= static_cast<size_t>(r);
+    }
+    return true;
+}
+constexpr int kReadThreads = 8;
+}  // namespace
+
+// Frames are fixed-size records (header + length_data bytes), so the frames of one call are
+// read with positioned reads from up to kReadThreads threads at once: one reader of
+// page-cached 1 MB frames moved about 4.6 GB/s, which was what bound the command line's
+// file-to-ISF rate. The same checks as src/video_reader.cpp:240-284 (a header and a data
+// block per frame); the file position advances by the frames read.
 extern "C" int ddm_movie_read(ddm_movie *m, void *dst, int count) {
     if (!m || !dst || count < 0) return ddm::fail(DDM_ERR_INVALID_ARG, "ddm_movie_read: bad argument");
-    unsigned char hdr[240];
     unsigned char *out = static_cast<unsigned char *>(dst);
-    for (int i = 0; i < count; i++) {  // src/video_reader.cpp:240-284
-        if (std::fread(hdr, m->header_len, 1, m->f) != 1)
-            return ddm::fail(DDM_ERR_IO, "[.moviefile Read Error] Corrupted header at offset " +
-                                             std::to_string(std::ftell(m->f)));
-        if (std::fread(out + size_t(i) * m->length_data, m->length_data, 1, m->f) != 1)
-            return ddm::fail(DDM_ERR_IO, "[.moviefile Read Error] Corrupted data at offset " +
-                                             std::to_string(std::ftell(m->f)));
+    const int fd = fileno(m->f);
+    const long long rec = m->header_len + static_cast<long long>(m->length_data);
+    long long bad_header = -1, bad_data = -1;  // offset of the first record that failed
+    const int nt = std::max(1, std::min(count, kReadThreads));
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int i = 0; i < count; i++) {
+        unsigned char hdr[240];
+        const long long at = m->pos + i * rec;
+        const bool hok = read_at(fd, hdr, static_cast<size_t>(m->header_len), at);
+        const bool dok = hok && read_at(fd, out + size_t(i) * m->length_data, m->length_data, at + m->header_len);
+        if (!hok || !dok) {
+#pragma omp critical(ddm_movie_read_error)
+            {
+                long long &b = hok ? bad_data : bad_header;
+                const long long off = hok ? at + m->header_len : at;
+                if (b < 0 || off < b) b = off;
+            }
+        }
     }
+    if (bad_header >= 0 && (bad_data < 0 || bad_header < bad_data))
+        return ddm::fail(DDM_ERR_IO, "[.moviefile Read Error] Corrupted header at offset " + std::to_string(bad_header));
+    if (bad_data >= 0)
+        return ddm::fail(DDM_ERR_IO, "[.moviefile Read Error] Corrupted data at offset " + std::to_string(bad_data));
+    m->pos += count * rec;
     return DDM_OK;
 }
 

@@ -157,6 +157,11 @@ class Engine:
     def wait_isf(self) -> None:
         check(lib().ddm_wait_isf(self._h))
 
+    def wait_frames_copied(self, back: int = 1) -> None:
+        """Block until the host frames of the submit call `back` calls before the last have
+        been copied to the device (their buffer may be refilled)."""
+        check(lib().ddm_wait_frames_copied(self._h, int(back)))
+
     def set_async_depth(self, depth: int) -> None:
         """Keep depth - 1 finalize_async results in flight (2..8; default 2): each call then
         returns once the result of depth - 1 calls before is in its buffer, so the caller

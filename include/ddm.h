@@ -129,6 +129,13 @@ int ddm_close(ddm_engine *e);
  * engine's stream. */
 int ddm_submit_frames(ddm_engine *e, const void *frames, int count, int on_device);
 
+/* Block until the host frames of the submit call `back` calls before the last (0 = the last
+ * call, at most 7) have been copied to the device, so that buffer may be refilled while the
+ * engine still transforms and pairs them: a reader that alternates two buffers calls it with
+ * back = 1 before refilling the buffer of the call before last. Returns at once for calls
+ * that read device memory or do not exist. */
+int ddm_wait_frames_copied(ddm_engine *e, int back);
+
 /* Queue the remaining pairs (compat tail, src/DDM.cu:830-843) and the masked azimuthal
  * average of every (scale, tile, lambda, tau) bin; the result is ready for
  * ddm_read_isf. Replaces combineAccumulators + analyse_accums + analyseFFTDevice

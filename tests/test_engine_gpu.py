@@ -129,6 +129,35 @@ def test_device_and_host_submission_identical():
     assert np.array_equal(a, b)
 
 
+def test_two_pinned_buffers_refilled_after_wait_frames_copied():
+    """A reader that alternates two pinned buffers, refilling each after
+    ddm_wait_frames_copied(1) (the command line's file loop), gives the same ISF as
+    submitting every chunk from its own buffer; `back` outside 0..7 is an argument error."""
+    import torch
+    frames = media.synth_video(19, 128, 128, 120, 60, step_var=1.0)
+    kw = dict(frame_width=128, frame_height=128, scales=[128, 64], taus=[1, 2, 3, 7, 19, 40],
+              lambdas=[3.0, 6.0, 12.0, 24.0], chunk_frames=20, estimator="unbiased")
+    with Engine(EngineConfig(**kw)) as eng:
+        for k in range(6):
+            eng.submit(frames[20 * k:20 * k + 20].copy())
+        eng.finalize()
+        want = eng.isf()
+    with Engine(EngineConfig(**kw)) as eng:
+        bufs = [torch.empty((20, 128, 128), dtype=torch.uint8).pin_memory() for _ in range(2)]
+        bufs[0].copy_(torch.from_numpy(frames[0:20]))
+        for k in range(6):
+            eng.submit(bufs[k % 2].data_ptr(), 20, False)
+            if k < 5:
+                eng.wait_frames_copied(1)
+                bufs[(k + 1) % 2].copy_(torch.from_numpy(frames[20 * (k + 1):20 * (k + 2)]))
+        eng.finalize()
+        got = eng.isf()
+        for bad in (-1, 8):
+            with pytest.raises(DDMError):
+                eng.wait_frames_copied(bad)
+    assert np.array_equal(got, want)
+
+
 def test_static_video_is_zero_and_intensity_scales_quadratically():
     static = np.repeat(media.synth_video(4, 64, 64, 1, 20, noise_sd=0.0), 12, axis=0)
     isf, _, _ = engine_run(static, [64, 32], [1, 3], [4.0, 8.0], estimator="unbiased", C=4)

@@ -137,6 +137,32 @@ def test_movie_u16_roundtrip(tmp_path):
     lib().ddm_movie_close(h)
 
 
+def test_movie_reads_in_parallel_across_calls(tmp_path):
+    """Frames are read with positioned reads from several threads: consecutive calls of 13 and
+    27 frames return the file's frames in order, and a file cut inside a frame's data reports
+    the record's offset."""
+    fr = media.synth_video(7, 40, 24, 40, 10)
+    p = tmp_path / "c.movie"
+    media.write_movie(p, fr)
+    from cuda_multiddm_b200._lib import MovieInfo
+    h, info = C.c_void_p(), MovieInfo()
+    assert lib().ddm_movie_open(str(p).encode(), 0, C.byref(h), C.byref(info)) == 0
+    a = np.zeros((13, 24, 40), np.uint8)
+    b = np.zeros((27, 24, 40), np.uint8)
+    assert lib().ddm_movie_read(h, a.ctypes.data, 13) == 0
+    assert lib().ddm_movie_read(h, b.ctypes.data, 27) == 0
+    assert np.array_equal(np.concatenate([a, b]), fr)
+    lib().ddm_movie_close(h)
+    rec = 172 + 40 * 24
+    q = tmp_path / "d.movie"
+    q.write_bytes(p.read_bytes()[:10 * rec + 172 + 100])  # frame 10 cut inside its data
+    assert lib().ddm_movie_open(str(q).encode(), 0, C.byref(h), C.byref(info)) == 0
+    c = np.zeros((12, 24, 40), np.uint8)
+    assert lib().ddm_movie_read(h, c.ctypes.data, 12) == 7  # DDM_ERR_IO
+    assert f"Corrupted data at offset {10 * rec + 172}" in lib().ddm_last_error().decode()
+    lib().ddm_movie_close(h)
+
+
 def test_synth_deterministic_and_physical():
     a = media.synth_video(1001, 64, 64, 4, 20)
     b = media.synth_video(1001, 64, 64, 4, 20)
